@@ -1,0 +1,252 @@
+/*
+ * wos_b200.h — C ABI of the B200 walk-on-spheres library (libwos_b200.so).
+ *
+ * Plain C types only: host or device pointers and sizes, int status codes,
+ * no exceptions across the boundary.  One CUDA stream per context.  Each
+ * entry point names the reference interface it replaces (paths inside the
+ * zhouzh721/walk-on-spheres sources).
+ *
+ * Status: every function returning int returns WOS_OK (0) on success; on
+ * failure the message is available from wos_last_error(ctx) (or
+ * wos_last_global_error() when no context exists).
+ */
+#ifndef WOS_B200_H
+#define WOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WOS_B200_ABI_VERSION 1
+
+/* status codes */
+enum {
+    WOS_OK = 0,
+    WOS_ERR_INVALID = 1,   /* bad argument or state */
+    WOS_ERR_CUDA = 2,      /* CUDA runtime error */
+    WOS_ERR_MESH = 3,      /* mesh file or mesh content rejected (src/mesh.cpp:17-22) */
+    WOS_ERR_DEVICE = 4,    /* a kernel raised its error word (bounded loop ran out) */
+    WOS_ERR_IO = 5         /* output file could not be written */
+};
+
+/* Equation kinds in the order of the reference registry
+ * (src/equations/equations.hpp:26-31). */
+enum {
+    WOS_EQ_LAPLACE = 0,
+    WOS_EQ_POISSON = 1,
+    WOS_EQ_SCREENED_POISSON = 2,
+    WOS_EQ_HELMHOLTZ = 3
+};
+
+/* Source sampling modes (include/wos/source_mode.hpp:5-9). */
+enum { WOS_SOURCE_UNIFORM = 0, WOS_SOURCE_GREEN = 1 };
+
+/* Walk methods.
+ *  PLAIN_FP64: the reference estimator (include/wos/wos.hpp:54-191) in FP64,
+ *    every walk of a point on the point's own xoshiro256++ streams in the
+ *    reference's order (include/wos/runner.hpp:208-222); matches the
+ *    reference run to rounding of the transcendental functions.
+ *  FAST_FP32: FP32 distance / closest-point / sphere-step arithmetic with an
+ *    FP64 re-projection inside the epsilon shell, FP64 estimator sums, and
+ *    counter-based Philox streams per (grid point, walk); statistically
+ *    equivalent, not bitwise equal, to PLAIN_FP64.
+ *  FAST_FP64: the FAST_FP32 scheduling with FP64 arithmetic throughout
+ *    (the same counter-based streams). */
+enum { WOS_METHOD_PLAIN_FP64 = 0, WOS_METHOD_FAST_FP32 = 1, WOS_METHOD_FAST_FP64 = 2 };
+
+/* Location codes (include/wos/inside.hpp:8-13). */
+enum { WOS_OUTSIDE = 0, WOS_INSIDE = 1, WOS_BOUNDARY = 2, WOS_INDETERMINATE = 3 };
+
+typedef struct wos_context wos_context;
+
+/* Cartesian grid (include/wos/grid.hpp:5-10); coordinate i is
+ * min + (max-min)*i/(N-1) (grid.hpp:12-18).  2D grids use Nz = 1. */
+typedef struct {
+    int Nx, Ny, Nz;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+} wos_grid;
+
+/* Solver arguments: the scalars of the reference registry entry
+ * (src/equations/equations.hpp:8-16) plus the walk method. */
+typedef struct {
+    int equation;          /* WOS_EQ_* */
+    int source_mode;       /* WOS_SOURCE_* (poisson, screened_poisson) */
+    double alpha;          /* screened_poisson coefficient */
+    int N_walks;           /* walks per inside point (>= 1) */
+    double epsilon;        /* requested stopping distance; screened_poisson clamps it to
+                              min(epsilon, 0.05/alpha) (src/equations/screened_poisson.cpp:22-38) */
+    int max_steps;         /* walk step cap (>= 1) */
+    int max_ray_attempts;  /* 3D inside-test ray budget (>= 3) */
+    uint64_t seed;         /* --seed: per-point streams are splitmix64(seed ^ splitmix64(index)) */
+    int method;            /* WOS_METHOD_* */
+} wos_params;
+
+/* Run diagnostics (include/wos/runner.hpp:240-283 plus timings). */
+typedef struct {
+    long long inside_points;
+    long long max_steps_hits;
+    long long ambiguous_ray_retries;
+    long long indeterminate_points;
+    long long total_walks;
+    long long total_steps;          /* sum of steps over all walks */
+    double sum_variance;            /* over inside points, grid order */
+    double sum_standard_error;
+    double sum_mean_steps;
+    double effective_epsilon;
+    float classify_ms;              /* device time of the classification kernel */
+    float walk_ms;                  /* device time of the walk kernel(s) */
+    float total_ms;                 /* device time of the whole solve */
+} wos_counters;
+
+/* ---------------------------------------------------------------- context */
+
+/* Create a context on CUDA device `device` with its own stream. */
+int wos_context_create(int device, wos_context **out);
+void wos_context_destroy(wos_context *ctx);
+const char *wos_last_error(const wos_context *ctx);
+const char *wos_last_global_error(void);
+int wos_abi_version(void);
+
+/* ------------------------------------------------------------------- mesh */
+
+/* Upload a boundary mesh and build its device BVHs.  Replaces the mesh
+ * broadcast and BVH build/broadcast of include/wos/runner.hpp:28-77
+ * (load_mesh src/mesh.cpp:76-270, build_bvh src/bvh.cpp:234-253).
+ *  dim 2: prims = n_prims segments (2 vertex indices each, 0-based),
+ *         boundary_ids = the `l` record of each segment (may be NULL: all 0);
+ *  dim 3: prims = n_prims triangles (3 vertex indices each).
+ *  leaf_size: maximum primitives per BVH leaf, 2..8 (0 selects the default 4,
+ *  the reference's LEAF_SIZE, src/bvh.cpp:15).
+ * Rejects zero-length segments and degenerate triangles like
+ * src/mesh.cpp:239-267. */
+int wos_set_mesh(wos_context *ctx, int dim, const double *verts, int n_verts, const int *prims,
+                 int n_prims, const int *boundary_ids, int leaf_size);
+
+/* Load an OBJ file with the reference's reader semantics (src/mesh.cpp:51-270:
+ * `v`, `l` polylines auto-closed with one boundary_id per record, `f`
+ * triangles only) and upload it as wos_set_mesh does. */
+int wos_load_obj(wos_context *ctx, const char *path, int leaf_size);
+
+/* Mesh bounding box {xmin, xmax, ymin, ymax, zmin, zmax} (src/mesh.cpp:297-322)
+ * and dimension of the current mesh. */
+int wos_mesh_info(const wos_context *ctx, int *dim, int *n_prims, double bbox[6]);
+
+/* Fill `grid` with Nx x Ny x Nz points over the mesh bounding box, as
+ * include/wos/runner.hpp:83-85 does. */
+int wos_grid_over_mesh(const wos_context *ctx, int Nx, int Ny, int Nz, wos_grid *grid);
+
+/* ------------------------------------------------------------------ solve */
+
+/* Per-grid-point WoS sweep: the loop body of include/wos/runner.hpp:157-236
+ * for every point of `grid` (start point, inside/outside/boundary
+ * classification, boundary value, wos_run).  Output arrays are HOST arrays of
+ * Nx*Ny*Nz elements in row-major (i, j, k) order (include/wos/field_3D.hpp:
+ * 9-31); any of them may be NULL.  Values of outside / indeterminate points
+ * are NaN, boundary points get {g(nearest), 0, 0, 0} (runner.hpp:196-206).
+ * Blocks until the results are on the host. */
+int wos_solve_grid(wos_context *ctx, const wos_params *params, const wos_grid *grid,
+                   double *mean, double *variance, double *standard_error, double *mean_steps,
+                   uint8_t *location, wos_counters *counters);
+
+/* As wos_solve_grid, but the output pointers are DEVICE pointers on the
+ * context's device (any may be NULL) and nothing is copied to the host;
+ * counters (if given) are filled after the solve completes. */
+int wos_solve_grid_device(wos_context *ctx, const wos_params *params, const wos_grid *grid,
+                          double *mean, double *variance, double *standard_error,
+                          double *mean_steps, uint8_t *location, wos_counters *counters);
+
+/* The point-level operator: wos_run (include/wos/wos.hpp:160-191) with
+ * get_start_point (wos.hpp:42-52) and classification for `n` arbitrary start
+ * points (host array n*dim).  point_index[i] plays the role of the grid
+ * linear index in the seeding (runner.hpp:163-168); NULL uses i. */
+int wos_solve_points(wos_context *ctx, const wos_params *params, const double *points,
+                     const uint64_t *point_index, long long n, double *mean, double *variance,
+                     double *standard_error, double *mean_steps, uint8_t *location,
+                     wos_counters *counters);
+
+/* -------------------------------------------------- kernel-level checks */
+
+/* First `count` outputs of the device xoshiro256++ stream PRNG(seeds[s])
+ * (include/wos/prng.hpp:14-24, src/prng.cpp:6-15) for every seed:
+ * out[s*count + i]. */
+int wos_prng_u64(wos_context *ctx, const uint64_t *seeds, long long n_seeds, int count,
+                 uint64_t *out);
+
+/* Closest boundary point of each query (bvh_npq, src/bvh.cpp:295-387) on the
+ * device.  precision 64: the FP64 traversal used by PLAIN_FP64, the
+ * classification and the epsilon shell; 32: the FP32 traversal of FAST_FP32
+ * (distances then carry FP32 rounding).  boundary_id may be NULL. */
+int wos_closest_points(wos_context *ctx, int precision, const double *points, long long n,
+                       double *dist, double *nearest, int *boundary_id);
+
+/* Scheduling overrides of the FAST methods (no reference counterpart):
+ * walks per task and persistent grid size; <= 0 restores the automatic
+ * choice.  Used by the benchmark's tuner. */
+int wos_set_tuning(wos_context *ctx, int chunk, int blocks);
+
+/* ------------------------------------------------------- registry (drop-in) */
+
+/* One entry of the equation registry with the reference's run signature
+ * (src/equations/equations.hpp:7-17): load the OBJ mesh, sweep the grid over
+ * its bounding box on the GPU, print the reference's diagnostics and write
+ * the HDF5 result (include/wos/hdf5_io.hpp layout).  source_mode is the
+ * integer value of wos::SourceMode.  Returns 0 on success, 1 on failure, as
+ * the reference does.  The walk method is PLAIN_FP64 unless the environment
+ * variable WOS_B200_METHOD is "fast" (FAST_FP32) or "fast64" (FAST_FP64). */
+typedef int (*wos_run_fn)(int rank, int size, const char *mesh_filename,
+                          const char *output_filename, int Nx, int Ny, int Nz, int N_walks,
+                          double epsilon, int max_steps, int max_ray_attempts, uint64_t seed,
+                          double alpha, int source_mode);
+
+typedef struct {
+    const char *name;
+    wos_run_fn run_2D;
+    wos_run_fn run_3D;
+} wos_equation_entry;
+
+/* The registry: laplace, poisson, screened_poisson, helmholtz
+ * (src/equations/equations.hpp:26-31). */
+const wos_equation_entry *wos_equation_registry(int *count);
+
+/* ------------------------------------------------ host-only (no GPU needed) */
+
+/* Read an OBJ boundary mesh (load_mesh, src/mesh.cpp:76-270).  Call once with
+ * null arrays to get dim / n_verts / n_prims, then with arrays of
+ * n_verts*dim doubles, n_prims*dim ints and (2D) n_prims ints.  On failure
+ * returns WOS_ERR_MESH and copies the reference-formatted message
+ * ("Mesh <path>[:<line>]: <what>") into `error`. */
+int wos_read_obj(const char *path, int *dim, int *n_verts, int *n_prims, double *verts,
+                 int *prims, int *boundary_ids, char *error, int error_capacity);
+
+/* Host BVH build (the device layout's FP64 part; build_bvh, src/bvh.cpp:234-253):
+ * depth D, node boxes (2^(D+1) nodes x 2*dim doubles: lo then hi, node id 0
+ * unused, 1-based heap order) and the leaf-slot primitive order (n_prims).
+ * Pass null arrays to get the depth only. */
+int wos_build_bvh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                  int leaf_size, int *depth, double *node_boxes, int *order);
+
+/* Write a result file with the reference's HDF5 layout (wos_write_hdf5,
+ * include/wos/hdf5_io.hpp:15-338): /mean /variance /standard_error
+ * /mean_steps (f64 [Nx,Ny,Nz]), /location (u8), /x /y /z and the /metadata
+ * scalars (ray counters when write_ray_metadata, alpha and source_mode when
+ * write_source_metadata). */
+int wos_write_hdf5(const char *path, const wos_grid *grid, const double *mean,
+                   const double *variance, const double *standard_error,
+                   const double *mean_steps, const uint8_t *location, int N_walks,
+                   double epsilon, int max_steps, long long max_steps_hits,
+                   int write_ray_metadata, int max_ray_attempts, long long ambiguous_ray_retries,
+                   long long indeterminate_points, uint64_t seed, int write_source_metadata,
+                   double alpha, int source_mode);
+
+/* Peek the mesh dimension (2 if the first primitive record is `l`, 3 if `f`),
+ * src/mesh.cpp:51-74.  Returns 2, 3, or 0 on error. */
+int wos_peek_mesh_dim(const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WOS_B200_H */

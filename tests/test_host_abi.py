@@ -1,0 +1,218 @@
+"""CPU tests of libwos_b200's C ABI and host logic (no GPU needed): symbol
+exports, the OBJ reader against the reference loader (src/mesh.cpp), the host
+BVH build, and the HDF5 result writer against the pure-Python reader (itself
+checked on a libhdf5-written file)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from walk_on_spheres_b200 import _lib, h5lite, meshes
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "wos_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b(wos_[a-z0-9_]+)\s*\(", text))
+    return sorted(n for n in names if not n.endswith("_fn"))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert L.wos_abi_version() == 1
+    assert set(_lib.SIGNATURES) <= set(names)
+
+
+def test_registry_names():
+    from walk_on_spheres_b200.solver import registry
+    assert [e.name for e in registry()] == ["laplace", "poisson", "screened_poisson", "helmholtz"]
+
+
+def read_obj(path):
+    L = _lib.lib()
+    f = L.wos_read_obj
+    f.restype = C.c_int
+    dim, nv, npr = C.c_int(), C.c_int(), C.c_int()
+    err = C.create_string_buffer(512)
+    rc = f(str(path).encode(), C.byref(dim), C.byref(nv), C.byref(npr), None, None, None, err, 512)
+    if rc:
+        return rc, err.value.decode()
+    verts = np.zeros((nv.value, dim.value))
+    prims = np.zeros((npr.value, dim.value), dtype=np.int32)
+    bids = np.zeros(npr.value, dtype=np.int32)
+    f(str(path).encode(), C.byref(dim), C.byref(nv), C.byref(npr),
+      verts.ctypes.data_as(C.c_void_p), prims.ctypes.data_as(C.c_void_p),
+      bids.ctypes.data_as(C.c_void_p), err, 512)
+    return 0, (dim.value, verts, prims, bids)
+
+
+BAD_OBJS = {
+    "no_vertices.obj": "l 1 2\n",
+    "short_polyline.obj": "v 0 0\nv 1 0\nl 1\n",
+    "quad.obj": "v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nf 1 2 3 4\n",
+    "index_range.obj": "v 0 0\nv 1 0\nv 1 1\nl 1 2 9\n",
+    "zero_index.obj": "v 0 0\nv 1 0\nl 0 1\n",
+    "bad_index.obj": "v 0 0\nv 1 0\nl 1 x2\n",
+    "zero_length.obj": "v 0 0\nv 0 0\nv 1 0\nl 1 2 3\n",
+    "degenerate.obj": "v 0 0 0\nv 1 0 0\nv 2 0 0\nv 0 1 0\nf 1 2 3\nf 1 2 4\n",
+    "malformed_vertex.obj": "v 0\nv 1 0\nl 1 2\n",
+    "nonfinite.obj": "v 0 0 inf\nv 1 0 0\nv 0 1 0\nf 1 2 3\n",
+    "no_prims.obj": "v 0 0\nv 1 1\n",
+    "bad_face.obj": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 #c\n",
+}
+
+GOOD_OBJS = {
+    # open polyline auto-closed, comments, slash references, second loop
+    "open.obj": "# c\nv 0 0\nv 1 0\nv 1 1 # z-less\nl 1 2/5 3\nv 3 3\nv 4 3\nv 4 4\nl 4 5 6 4\n",
+    "tri.obj": "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf 1 3 2\nf 1 2 4\nf 2 3 4\nf 1 4 3\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(BAD_OBJS))
+def test_obj_errors_match_reference(tmp_path, reference, name):
+    p = tmp_path / name
+    p.write_text(BAD_OBJS[name])
+    rc, msg = read_obj(p)
+    assert rc == 3
+    with pytest.raises(ValueError) as e:
+        reference.load_mesh(str(p))
+    assert msg == str(e.value)
+
+
+@pytest.mark.parametrize("name", sorted(GOOD_OBJS))
+def test_obj_reader_matches_reference(tmp_path, reference, name):
+    p = tmp_path / name
+    p.write_text(GOOD_OBJS[name])
+    rc, (dim, verts, prims, bids) = read_obj(p)
+    assert rc == 0
+    rdim, rv, rp, rb = reference.load_mesh(str(p))
+    assert dim == rdim
+    assert np.array_equal(verts, rv)
+    assert np.array_equal(prims, rp)
+    if dim == 2:
+        assert np.array_equal(bids, rb)
+
+
+def test_generated_meshes_round_trip(tmp_path):
+    for m in (meshes.annulus(), meshes.uv_sphere(lon=16, lat=8)):
+        p = meshes.write_obj(m, tmp_path / f"m{m.dim}.obj")
+        rc, (dim, verts, prims, bids) = read_obj(p)
+        assert rc == 0 and dim == m.dim
+        assert np.array_equal(verts, m.verts)
+        assert np.array_equal(prims, m.prims)
+        if dim == 2:
+            assert np.array_equal(bids, m.boundary_ids)
+
+
+def build_bvh(m, leaf):
+    L = _lib.lib()
+    f = L.wos_build_bvh
+    f.restype = C.c_int
+    verts = np.ascontiguousarray(m.verts)
+    prims = np.ascontiguousarray(m.prims, dtype=np.int32)
+    d = C.c_int()
+    assert f(m.dim, verts.ctypes.data_as(C.c_void_p), verts.shape[0],
+             prims.ctypes.data_as(C.c_void_p), prims.shape[0], leaf, C.byref(d), None, None) == 0
+    D = d.value
+    boxes = np.zeros((2 ** (D + 1), 2 * m.dim))
+    order = np.zeros(m.n_prims, dtype=np.int32)
+    f(m.dim, verts.ctypes.data_as(C.c_void_p), verts.shape[0], prims.ctypes.data_as(C.c_void_p),
+      prims.shape[0], leaf, C.byref(d), boxes.ctypes.data_as(C.c_void_p),
+      order.ctypes.data_as(C.c_void_p))
+    return D, boxes, order
+
+
+@pytest.mark.parametrize("leaf", [2, 3, 4, 6, 8])
+@pytest.mark.parametrize("mname", ["annulus", "sphere", "circle1000"])
+def test_host_bvh_invariants(leaf, mname):
+    m = {"annulus": meshes.annulus(), "sphere": meshes.uv_sphere(lon=20, lat=11),
+         "circle1000": meshes.circle(segments=1000)}[mname]
+    D, boxes, order = build_bvh(m, leaf)
+    n, d = m.n_prims, m.dim
+    assert sorted(order.tolist()) == list(range(n))          # every primitive once
+    assert -(-n // 2 ** D) <= leaf                            # ceil(n / 2^D) fits a leaf
+    assert D == 0 or -(-n // 2 ** (D - 1)) > leaf             # and D is the smallest such depth
+    lo_p = m.verts[m.prims].min(axis=1)
+    hi_p = m.verts[m.prims].max(axis=1)
+    for j in range(2 ** D):
+        b, e = (j * n) >> D, ((j + 1) * n) >> D
+        node = 2 ** D + j
+        sl = order[b:e]
+        assert e > b
+        assert np.array_equal(boxes[node, :d], lo_p[sl].min(axis=0))
+        assert np.array_equal(boxes[node, d:], hi_p[sl].max(axis=0))
+    for i in range(1, 2 ** D):                                # parents bound children
+        assert np.array_equal(boxes[i, :d], np.minimum(boxes[2 * i, :d], boxes[2 * i + 1, :d]))
+        assert np.array_equal(boxes[i, d:], np.maximum(boxes[2 * i, d:], boxes[2 * i + 1, d:]))
+
+
+def test_mesh_validation_rejects_degenerate():
+    L = _lib.lib()
+    verts = np.array([[0.0, 0.0], [0.0, 0.0], [1.0, 0.0]])
+    prims = np.array([[0, 1], [1, 2], [2, 0]], dtype=np.int32)
+    L.wos_build_bvh.restype = C.c_int
+    rc = L.wos_build_bvh(2, verts.ctypes.data_as(C.c_void_p), 3, prims.ctypes.data_as(C.c_void_p),
+                         3, 0, None, None, None)
+    assert rc == 3
+
+
+SPECIMEN = Path(np.__file__).resolve().parents[1] / "scipy" / "io" / "matlab" / "tests" / \
+    "data" / "testhdf5_7.4_GLNX86.mat"
+
+
+@pytest.mark.skipif(not SPECIMEN.exists(), reason="libhdf5-written specimen not available")
+def test_h5lite_reads_libhdf5_file():
+    f = h5lite.read(SPECIMEN)
+    assert list(f) == ["/testdouble"]
+    assert np.allclose(f["/testdouble"].ravel(), np.arange(9) * np.pi / 4)
+
+
+def write_result(path, grid, fields, meta):
+    L = _lib.lib()
+    f = L.wos_write_hdf5
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.POINTER(_lib.Grid)] + [C.c_void_p] * 5 + [
+        C.c_int, C.c_double, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_longlong,
+        C.c_longlong, C.c_uint64, C.c_int, C.c_double, C.c_int]
+    return f(str(path).encode(), C.byref(grid),
+             *[a.ctypes.data_as(C.c_void_p) for a in fields], *meta)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_hdf5_result_layout(tmp_path, dim):
+    nx, ny, nz = 5, 4, (3 if dim == 3 else 1)
+    g = _lib.Grid(nx, ny, nz, -1.0, 1.0, -0.5, 0.5, (-2.0 if dim == 3 else 0.0),
+                  (2.0 if dim == 3 else 0.0))
+    rng = np.random.default_rng(dim)
+    n = nx * ny * nz
+    fields = [rng.standard_normal(n) for _ in range(4)] + [rng.integers(0, 4, n).astype(np.uint8)]
+    meta = (1234, 0.005, 1000, 17, int(dim == 3), 12, 5, 2, 2**64 - 5, 1, 10.0, 1)
+    assert write_result(tmp_path / "r.h5", g, fields, meta) == 0
+    f = h5lite.read(tmp_path / "r.h5")
+    names = ["mean", "variance", "standard_error", "mean_steps", "location"]
+    for k, a in zip(names, fields):
+        assert f["/" + k].shape == (nx, ny, nz)
+        assert np.array_equal(f["/" + k].ravel(), a)
+    assert f["/location"].dtype == np.uint8 and f["/mean"].dtype == np.float64
+    assert np.array_equal(f["/x"], [-1.0 + 2.0 * i / 4 for i in range(nx)])
+    assert f["/z"].shape == (nz,)
+    m = {k.split("/")[-1]: v for k, v in f.items() if k.startswith("/metadata/")}
+    assert m["N_walks"] == 1234 and m["N_walks"].dtype == np.int32
+    assert m["epsilon"] == 0.005 and m["max_steps"] == 1000
+    assert m["max_steps_hits"] == 17 and m["max_steps_hits"].dtype == np.int64
+    assert m["seed"] == 2**64 - 5 and m["seed"].dtype == np.uint64
+    assert m["alpha"] == 10.0 and m["source_mode"] == 1
+    assert ("ambiguous_ray_retries" in m) == (dim == 3)
+    if dim == 3:
+        assert m["max_ray_attempts"] == 12 and m["indeterminate_points"] == 2

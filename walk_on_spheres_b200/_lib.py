@@ -1,0 +1,113 @@
+"""ctypes binding of libwos_b200.so (the C ABI declared in include/wos_b200.h).
+
+The library is the only compute path: there is no CPU or PyTorch fallback.
+If the shared library is missing, importing the binding raises, and every
+solver call goes through the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("WOS_B200_LIB", PKG / "lib" / "libwos_b200.so"))
+
+WOS_OK = 0
+STATUS_NAMES = {0: "WOS_OK", 1: "WOS_ERR_INVALID", 2: "WOS_ERR_CUDA", 3: "WOS_ERR_MESH",
+                4: "WOS_ERR_DEVICE", 5: "WOS_ERR_IO"}
+
+
+class WosError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Grid(C.Structure):
+    """wos_grid (include/wos/grid.hpp:5-10)."""
+    _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("Nz", C.c_int),
+                ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+                ("ymax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double)]
+
+
+class Params(C.Structure):
+    """wos_params: the registry entry's scalars plus the walk method."""
+    _fields_ = [("equation", C.c_int), ("source_mode", C.c_int), ("alpha", C.c_double),
+                ("N_walks", C.c_int), ("epsilon", C.c_double), ("max_steps", C.c_int),
+                ("max_ray_attempts", C.c_int), ("seed", C.c_uint64), ("method", C.c_int)]
+
+
+class Counters(C.Structure):
+    """wos_counters (include/wos/runner.hpp:240-283 plus device timings)."""
+    _fields_ = [("inside_points", C.c_longlong), ("max_steps_hits", C.c_longlong),
+                ("ambiguous_ray_retries", C.c_longlong), ("indeterminate_points", C.c_longlong),
+                ("total_walks", C.c_longlong), ("total_steps", C.c_longlong),
+                ("sum_variance", C.c_double), ("sum_standard_error", C.c_double),
+                ("sum_mean_steps", C.c_double), ("effective_epsilon", C.c_double),
+                ("classify_ms", C.c_float), ("walk_ms", C.c_float), ("total_ms", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
+                     C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double,
+                     C.c_int)
+
+
+class EquationEntry(C.Structure):
+    """wos_equation_entry (src/equations/equations.hpp:7-17)."""
+    _fields_ = [("name", C.c_char_p), ("run_2D", RUN_FN), ("run_3D", RUN_FN)]
+
+
+# exported symbols of include/wos_b200.h with their signatures
+VP = C.c_void_p
+SIGNATURES = {
+    "wos_abi_version": (C.c_int, []),
+    "wos_context_create": (C.c_int, [C.c_int, C.POINTER(VP)]),
+    "wos_context_destroy": (None, [VP]),
+    "wos_last_error": (C.c_char_p, [VP]),
+    "wos_last_global_error": (C.c_char_p, []),
+    "wos_set_mesh": (C.c_int, [VP, C.c_int, VP, C.c_int, VP, C.c_int, VP, C.c_int]),
+    "wos_load_obj": (C.c_int, [VP, C.c_char_p, C.c_int]),
+    "wos_mesh_info": (C.c_int, [VP, C.POINTER(C.c_int), C.POINTER(C.c_int), VP]),
+    "wos_grid_over_mesh": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.POINTER(Grid)]),
+    "wos_solve_grid": (C.c_int, [VP, C.POINTER(Params), C.POINTER(Grid)] + [VP] * 5 +
+                       [C.POINTER(Counters)]),
+    "wos_solve_grid_device": (C.c_int, [VP, C.POINTER(Params), C.POINTER(Grid)] + [VP] * 5 +
+                              [C.POINTER(Counters)]),
+    "wos_solve_points": (C.c_int, [VP, C.POINTER(Params), VP, VP, C.c_longlong] + [VP] * 5 +
+                         [C.POINTER(Counters)]),
+    "wos_prng_u64": (C.c_int, [VP, VP, C.c_longlong, C.c_int, VP]),
+    "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
+    "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_equation_registry": (C.POINTER(EquationEntry), [C.POINTER(C.c_int)]),
+    "wos_peek_mesh_dim": (C.c_int, [C.c_char_p]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libwos_b200.so once; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m walk_on_spheres_b200.build` "
+                "(the CUDA library is required: there is no CPU fallback)")
+        handle = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(handle, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status: int, ctx=None) -> None:
+    if status != WOS_OK:
+        L = lib()
+        msg = (L.wos_last_error(ctx) if ctx else L.wos_last_global_error()) or b""
+        raise WosError(status, msg.decode(errors="replace"))

@@ -1,0 +1,58 @@
+// Internal state behind the opaque wos_context of include/wos_b200.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/wos_b200.h"
+#include "kernels.h"
+#include "scene_build.h"
+
+namespace wosb {
+
+// Grow-only device allocation.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n);
+    void release();
+};
+
+double effective_epsilon(const wos_params &p);
+
+}  // namespace wosb
+
+struct wos_context {
+    int device = 0;
+    int sms = 148;
+    size_t smem_optin = 0;
+    int cc_major = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string error;
+
+    bool has_mesh = false;
+    wosb::HostScene scene;
+    wosb::SceneView view{};
+
+    // scene
+    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, tri32;
+    // per solve
+    wosb::DeviceBuffer location, start, f_mean, f_var, f_se, f_steps, f_loc, partials, queue,
+        counters, points, index;
+    // kernel-level checks
+    wosb::DeviceBuffer scratch_a, scratch_b, scratch_c, scratch_d;
+
+    // tuning overrides (<= 0: automatic)
+    int chunk_override = 0;
+    int blocks_override = 0;
+
+    ~wos_context();
+    std::vector<wosb::DeviceBuffer *> all_buffers();
+    int upload_scene();
+    int run(const wos_params &p, const wosb::PointSet &ps, wosb::Fields out, wos_counters *c);
+    int fields_for(long long n, wosb::Fields &out);
+    int download(long long n, const wosb::Fields &dev, double *mean, double *variance, double *se,
+                 double *steps, uint8_t *loc);
+};

@@ -1,0 +1,464 @@
+// The reference's equation registry as device code.
+//
+// The reference's operator interface is a compile-time "Eq concept" resolved
+// in wos_sample (include/wos/wos.hpp:54-138): has_source / has_screening
+// flags, boundary(p[, boundary_id]), source(p), green(sphere, x, y),
+// green_mass(R), sample_green(sphere, rng), screening_factor(R) and, in 2D,
+// source_may_intersect(sphere).  Each struct below is one registry entry for
+// one dimension with exactly those members (src/equations/laplace.cpp:12-43,
+// poisson.cpp:15-118, screened_poisson.cpp:40-141, helmholtz.cpp:15-78);
+// Green kernels follow include/wos/poisson.hpp:12-51 and
+// include/wos/screened.hpp:14-156.
+//
+// Member functions are templates on the arithmetic type T: the exact path
+// instantiates them with double (expression shapes follow the reference so
+// they round identically), the fast path with float.  Random draws come from
+// an Rng with unit() in [0, 1) and unit_open() in (0, 1).
+#pragma once
+#include "special.cuh"
+
+namespace wosb {
+
+enum : int { kLaplace = 0, kPoisson = 1, kScreened = 2, kHelmholtz = 3 };
+enum : int { kUniform = 0, kGreen = 1 };
+
+template <typename T>
+struct V3 {
+    T x, y, z;
+};
+
+template <typename T>
+__device__ __forceinline__ T harmonic_y5(T x, T y, T z) {
+    // src/equations/laplace.cpp:30-36
+    const T r_sq = x * x + y * y;
+    const T y50 = z * (T(8) * z * z * z * z - T(40) * z * z * r_sq + T(15) * r_sq * r_sq);
+    const T y5m3 = (T(8) * z * z - r_sq) * y * (T(3) * x * x - y * y);
+    return y50 + T(4) * y5m3;
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ T dist(V3<T> a, V3<T> b) {
+    if (DIM == 2) return sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+    return sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z));
+}
+
+// Angles: the exact path forms theta in double and calls cos/sin like the
+// reference; the fast path uses sincospi on 2u (no range reduction).
+template <typename T>
+__device__ __forceinline__ void sincos_2pi(T u, T &s, T &c);
+template <>
+__device__ __forceinline__ void sincos_2pi<float>(float u, float &s, float &c) {
+    sincospif(2.0f * u, &s, &c);
+}
+template <>
+__device__ __forceinline__ void sincos_2pi<double>(double u, double &s, double &c) {
+    sincospi(2.0 * u, &s, &c);
+}
+
+// ---------------------------------------------------------------- sampling
+
+// Exit point on the sphere, src/wos.cpp:9-30.
+template <int DIM, bool EXACT, typename T, class Rng>
+__device__ __forceinline__ V3<T> sphere_step(V3<T> c, T R, Rng &rng) {
+    if (DIM == 2) {
+        if constexpr (EXACT) {
+            const double theta = rng.unit() * 2 * kPi;
+            return V3<T>{c.x + R * cos(theta), c.y + R * sin(theta), T(0)};
+        }
+        T s, co;
+        sincos_2pi<T>(rng.unit(), s, co);
+        return V3<T>{c.x + R * co, c.y + R * s, T(0)};
+    } else {
+        const T u = rng.unit();
+        const T v = rng.unit();
+        const T z = T(2) * u - T(1);
+        const T r = sqrt(T(1) - z * z);
+        if constexpr (EXACT) {
+            const double phi = 2 * kPi * v;
+            return V3<T>{c.x + R * r * cos(phi), c.y + R * r * sin(phi), c.z + R * z};
+        }
+        T s, co;
+        sincos_2pi<T>(v, s, co);
+        return V3<T>{c.x + R * r * co, c.y + R * r * s, c.z + R * z};
+    }
+}
+
+// Uniform point in the ball, src/wos.cpp:33-56.
+template <int DIM, bool EXACT, typename T, class Rng>
+__device__ __forceinline__ V3<T> ball_sample(V3<T> c, T R, Rng &rng) {
+    if (DIM == 2) {
+        const T u = rng.unit();
+        const T r = R * sqrt(rng.unit_open());
+        if constexpr (EXACT) {
+            const double theta = u * 2 * kPi;
+            return V3<T>{c.x + r * cos(theta), c.y + r * sin(theta), T(0)};
+        }
+        T s, co;
+        sincos_2pi<T>(u, s, co);
+        return V3<T>{c.x + r * co, c.y + r * s, T(0)};
+    } else {
+        const T u = rng.unit();
+        const T v = rng.unit();
+        const T w = rng.unit_open();
+        const T z = T(2) * u - T(1);
+        const T surf = sqrt(T(1) - z * z);
+        const T vol = R * cbrt(w);
+        if constexpr (EXACT) {
+            const double phi = 2 * kPi * v;
+            return V3<T>{c.x + vol * surf * cos(phi), c.y + vol * surf * sin(phi),
+                         c.z + vol * z};
+        }
+        T s, co;
+        sincos_2pi<T>(v, s, co);
+        return V3<T>{c.x + vol * surf * co, c.y + vol * surf * s, c.z + vol * z};
+    }
+}
+
+// Point at `radius` from c in a uniform direction (the angular part of the
+// Green samplers, src/equations/poisson.cpp:62-72 / :105-117).
+template <int DIM, bool EXACT, typename T, class Rng>
+__device__ __forceinline__ V3<T> direction_at(V3<T> c, T radius, Rng &rng) {
+    if (DIM == 2) {
+        const T u = rng.unit();
+        if constexpr (EXACT) {
+            const double angle = 2.0 * kPi * u;
+            return V3<T>{c.x + radius * cos(angle), c.y + radius * sin(angle), T(0)};
+        }
+        T s, co;
+        sincos_2pi<T>(u, s, co);
+        return V3<T>{c.x + radius * co, c.y + radius * s, T(0)};
+    } else {
+        const T z = T(2) * rng.unit() - T(1);
+        const T u = rng.unit();
+        const T xy = sqrt(T(1) - z * z);
+        if constexpr (EXACT) {
+            const double angle = 2.0 * kPi * u;
+            return V3<T>{c.x + radius * xy * cos(angle), c.y + radius * xy * sin(angle),
+                         c.z + radius * z};
+        }
+        T s, co;
+        sincos_2pi<T>(u, s, co);
+        return V3<T>{c.x + radius * xy * co, c.y + radius * xy * s, c.z + radius * z};
+    }
+}
+
+// ------------------------------------------------------------ Green kernels
+
+// include/wos/poisson.hpp:14-20, 22-24, 29-32, 34-41, 43-45, 47-51
+template <typename T>
+__device__ __forceinline__ T pg_green_2d(T R, T r) {
+    if (!(r > T(0)) || r > R || R <= T(0)) return T(NAN);
+    if (r == R) return T(0);
+    return log(R / r) / (T(2) * T(kPi));
+}
+template <typename T>
+__device__ __forceinline__ T pg_mass_2d(T R) { return R * R / T(4); }
+template <typename T, class Rng>
+__device__ __forceinline__ T pg_sample_radius_2d(T R, Rng &rng) {
+    const T u = rng.unit_open();
+    const T v = rng.unit_open();
+    return R * sqrt(u * v);
+}
+template <typename T>
+__device__ __forceinline__ T pg_green_3d(T R, T r) {
+    if (!(r > T(0)) || r > R || R <= T(0)) return T(NAN);
+    if (r == R) return T(0);
+    return (R - r) / (T(4) * T(kPi) * r * R);
+}
+template <typename T>
+__device__ __forceinline__ T pg_mass_3d(T R) { return R * R / T(6); }
+template <typename T, class Rng>
+__device__ __forceinline__ T pg_sample_radius_3d(T R, Rng &rng) {
+    T u = rng.unit_open(), v = rng.unit_open();
+    const T a = -log(u * v);
+    u = rng.unit_open();
+    v = rng.unit_open();
+    const T b = -log(u * v);
+    return R * a / (a + b);
+}
+
+// include/wos/screened.hpp:14-89
+template <typename T>
+__device__ __forceinline__ T sc_weight_2d(T alpha, T R) {
+    const T x = alpha * R;
+    if (x == T(0)) return T(1);
+    if (x < T(1e-3)) {
+        const T x2 = x * x;
+        return T(1) - x2 / T(4) + T(3) * x2 * x2 / T(64);
+    }
+    return exp(-log_i0(x));
+}
+template <typename T>
+__device__ __forceinline__ T sc_green_2d(T alpha, T R, T r) {
+    if (!(r > T(0)) || r > R || R <= T(0)) return T(NAN);
+    if (r == R) return T(0);
+    const T x = alpha * r, X = alpha * R;
+    if (X < T(1e-5)) return pg_green_2d(R, r);
+    const T la = log_k0(x);
+    const T lb = log_i0(x) + log_k0(X) - log_i0(X);
+    T delta = lb - la;
+    if (delta > T(0)) delta = T(0);
+    return exp(la) * (-expm1(delta)) / (T(2) * T(kPi));
+}
+template <typename T>
+__device__ __forceinline__ T sc_mass_2d(T alpha, T R) {
+    const T x = alpha * R;
+    if (x < T(1e-3)) {
+        const T x2 = x * x;
+        return R * R * (T(1) / T(4) - T(3) * x2 / T(64) + T(19) * x2 * x2 / T(2304));
+    }
+    return -expm1(-log_i0(x)) / (alpha * alpha);
+}
+template <typename T>
+__device__ __forceinline__ T sc_weight_3d(T alpha, T R) {
+    const T x = alpha * R;
+    if (x == T(0)) return T(1);
+    if (x < T(1e-3)) {
+        const T x2 = x * x;
+        return T(1) - x2 / T(6) + T(7) * x2 * x2 / T(360);
+    }
+    return T(2) * x * exp(-x) / (-expm1(T(-2) * x));
+}
+template <typename T>
+__device__ __forceinline__ T sc_green_3d(T alpha, T R, T r) {
+    if (!(r > T(0)) || r > R || R <= T(0)) return T(NAN);
+    if (r == R) return T(0);
+    const T x = alpha * r, X = alpha * R;
+    if (X < T(1e-5)) return pg_green_3d(R, r);
+    const T ratio = exp(-x) * (-expm1(T(-2) * (X - x))) / (-expm1(T(-2) * X));
+    return ratio / (T(4) * T(kPi) * r);
+}
+template <typename T>
+__device__ __forceinline__ T sc_mass_3d(T alpha, T R) {
+    const T x = alpha * R;
+    if (x < T(1e-3)) {
+        const T x2 = x * x;
+        return R * R * (T(1) / T(6) - T(7) * x2 / T(360) + T(31) * x2 * x2 / T(15120));
+    }
+    return (T(1) - sc_weight_3d(alpha, R)) / (alpha * alpha);
+}
+template <typename T>
+__device__ __forceinline__ T clamp_probability(T v) {
+    const T lo = (v < T(1)) ? v : T(1);
+    return (T(0) < lo) ? lo : T(0);
+}
+template <typename T, class Rng>
+__device__ __forceinline__ T sc_normal(Rng &rng) {
+    const T radius = sqrt(T(-2) * log(rng.unit_open()));
+    const T angle_u = rng.unit();
+    return radius * cos(T(2) * T(kPi) * angle_u);
+}
+
+// Rejection samplers of the screened Green radius (screened.hpp:103-156).
+// The reference loops until acceptance; here the loop is capped and the cap
+// raises `overflow` (acceptance rates are ~0.5 or higher, so 4096 proposals
+// are never used up in practice).
+constexpr int kRejectionCap = 4096;
+
+template <typename T, class Rng>
+__device__ __forceinline__ T sc_sample_radius_2d(T alpha, T R, Rng &rng, bool &overflow) {
+    const T X = alpha * R;
+    T r = R * T(0.5);
+    for (int it = 0; it < kRejectionCap; ++it) {
+        T acc;
+        if (X < T(2)) {
+            r = pg_sample_radius_2d(R, rng);
+            const T proposal = pg_green_2d(R, r);
+            acc = sc_green_2d(alpha, R, r) / proposal;
+        } else {
+            const T time = -log(rng.unit_open()) / (alpha * alpha);
+            r = sqrt(T(-4) * time * log(rng.unit_open()));
+            if (r >= R) continue;
+            const T x = alpha * r;
+            const T lr = log_i0(x) + log_k0(X) - log_i0(X) - log_k0(x);
+            acc = -expm1((lr < T(0)) ? lr : T(0));
+        }
+        if (rng.unit() < clamp_probability(acc)) return r;
+    }
+    overflow = true;
+    return r;
+}
+
+template <typename T, class Rng>
+__device__ __forceinline__ T sc_sample_radius_3d(T alpha, T R, Rng &rng, bool &overflow) {
+    const T X = alpha * R;
+    T r = R * T(0.5);
+    for (int it = 0; it < kRejectionCap; ++it) {
+        T acc;
+        if (X < T(2)) {
+            r = pg_sample_radius_3d(R, rng);
+            const T proposal = pg_green_3d(R, r);
+            acc = sc_green_3d(alpha, R, r) / proposal;
+        } else {
+            const T time = -log(rng.unit_open()) / (alpha * alpha);
+            const T scale = sqrt(T(2) * time);
+            const T x0 = scale * sc_normal<T>(rng);
+            const T x1 = scale * sc_normal<T>(rng);
+            const T x2 = scale * sc_normal<T>(rng);
+            r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+            if (r >= R) continue;
+            const T x = alpha * r;
+            acc = (-expm1(T(-2) * (X - x))) / (-expm1(T(-2) * X));
+        }
+        if (rng.unit() < clamp_probability(acc)) return r;
+    }
+    overflow = true;
+    return r;
+}
+
+// ---------------------------------------------------------------- equations
+
+// Volume of the ball (include/wos/wos.hpp:21-27).
+template <int DIM, typename T>
+__device__ __forceinline__ T ball_volume(T R) {
+    if (DIM == 2) return T(kPi) * R * R;
+    const T rc = R * R * R;
+    return T(4) * T(kPi) * rc / T(3);
+}
+
+// laplace (src/equations/laplace.cpp:12-43)
+template <int DIM>
+struct Laplace {
+    static constexpr bool kSource = false, kScreening = false;
+    template <typename T>
+    __device__ T boundary(V3<T> p, int bid) const {
+        if (DIM == 2) return bid == 0 ? p.x * p.x - p.y * p.y : T(0);
+        return harmonic_y5(p.x, p.y, p.z);
+    }
+    template <typename T>
+    __device__ T screening(T) const { return T(1); }
+};
+
+// poisson (src/equations/poisson.cpp:15-118): 2D uniform load f = 0.1 on the
+// disk of radius 0.15 at the origin with g = 0; 3D f = 0 (draws still
+// consumed) with the degree-5 harmonic boundary data.
+template <int DIM>
+struct Poisson {
+    static constexpr bool kSource = true, kScreening = false;
+    int mode;
+    double alpha;
+    template <typename T>
+    __device__ T boundary(V3<T> p, int) const {
+        if (DIM == 2) return T(0);
+        return harmonic_y5(p.x, p.y, p.z);
+    }
+    template <typename T>
+    __device__ bool may_intersect(V3<T> c, T R) const {
+        const T dx = c.x - T(0), dy = c.y - T(0);
+        const T reach = R + T(0.15);
+        return dx * dx + dy * dy <= reach * reach;
+    }
+    template <typename T>
+    __device__ T source(V3<T> p) const {
+        if (DIM == 3) return T(0);
+        const T dx = p.x - T(0), dy = p.y - T(0);
+        return dx * dx + dy * dy <= T(0.15) * T(0.15) ? T(0.1) : T(0);
+    }
+    template <typename T>
+    __device__ T green(T R, T r) const {
+        return DIM == 2 ? pg_green_2d(R, r) : pg_green_3d(R, r);
+    }
+    template <typename T>
+    __device__ T green_mass(T R) const {
+        return DIM == 2 ? pg_mass_2d(R) : pg_mass_3d(R);
+    }
+    template <typename T, class Rng>
+    __device__ T green_radius(T R, Rng &rng, bool &) const {
+        return DIM == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
+    }
+    template <typename T>
+    __device__ T screening(T) const { return T(1); }
+};
+
+// screened_poisson (src/equations/screened_poisson.cpp:40-141): 2D bump f = 5
+// on the disk of radius 0.5 at (0.45, 0), g = x^2 - y^2 on boundary 0,
+// weight 1/I0(alpha R); 3D has no source (weight alpha R / sinh(alpha R) only)
+// and the degree-5 harmonic boundary data.
+template <int DIM>
+struct Screened {
+    static constexpr bool kSource = (DIM == 2), kScreening = true;
+    int mode;
+    double alpha;
+    template <typename T>
+    __device__ T boundary(V3<T> p, int bid) const {
+        if (DIM == 2) return bid == 0 ? p.x * p.x - p.y * p.y : T(0);
+        return harmonic_y5(p.x, p.y, p.z);
+    }
+    template <typename T>
+    __device__ bool may_intersect(V3<T> c, T R) const {
+        const T dx = c.x - T(0.45), dy = c.y - T(0);
+        const T reach = R + T(0.5);
+        return dx * dx + dy * dy <= reach * reach;
+    }
+    template <typename T>
+    __device__ T source(V3<T> p) const {
+        if (DIM == 3) return T(0);
+        return sqrt((p.x - T(0.45)) * (p.x - T(0.45)) + p.y * p.y) <= T(0.5) ? T(5) : T(0);
+    }
+    template <typename T>
+    __device__ T green(T R, T r) const {
+        const T a = static_cast<T>(alpha);
+        return DIM == 2 ? sc_green_2d(a, R, r) : sc_green_3d(a, R, r);
+    }
+    template <typename T>
+    __device__ T green_mass(T R) const {
+        const T a = static_cast<T>(alpha);
+        return DIM == 2 ? sc_mass_2d(a, R) : sc_mass_3d(a, R);
+    }
+    template <typename T, class Rng>
+    __device__ T green_radius(T R, Rng &rng, bool &overflow) const {
+        const T a = static_cast<T>(alpha);
+        return DIM == 2 ? sc_sample_radius_2d(a, R, rng, overflow)
+                        : sc_sample_radius_3d(a, R, rng, overflow);
+    }
+    template <typename T>
+    __device__ T screening(T R) const {
+        const T a = static_cast<T>(alpha);
+        return DIM == 2 ? sc_weight_2d(a, R) : sc_weight_3d(a, R);
+    }
+};
+
+// helmholtz (src/equations/helmholtz.cpp:15-78), k = 1, g = 1, no source:
+// weight 1/J0(kR) in 2D and kR/sin(kR) in 3D.
+template <int DIM>
+struct Helmholtz {
+    static constexpr bool kSource = false, kScreening = true;
+    template <typename T>
+    __device__ T boundary(V3<T>, int) const { return T(1); }
+    template <typename T>
+    __device__ T screening(T R) const {
+        const T prod = R * T(1);
+        if (prod < T(1e-8)) return T(1);
+        return DIM == 2 ? T(1) / bessel_j0(prod) : prod / sin(prod);
+    }
+};
+
+// One iteration of the walk loop body before the closest-point query
+// (include/wos/wos.hpp:69-115): the source contribution of the current ball,
+// the screening weight, then the step to the sphere.  Returns the new point.
+template <int DIM, bool EXACT, typename T, class Eq, class WalkRng, class SrcRng>
+__device__ __forceinline__ V3<T> walk_body(const Eq &eq, V3<T> p, T R, T &sample, T &weight,
+                                           WalkRng &walk, SrcRng &src, bool &overflow) {
+    if constexpr (Eq::kSource) {
+        bool may = true;
+        if (DIM == 2) may = eq.may_intersect(p, R);
+        if (may) {
+            if (eq.mode == kGreen) {
+                const T radius = eq.green_radius(R, src, overflow);
+                const V3<T> sp = direction_at<DIM, EXACT, T>(p, radius, src);
+                const T f = eq.source(sp);
+                if (f != T(0)) sample += weight * eq.green_mass(R) * f;
+            } else {
+                const V3<T> sp = ball_sample<DIM, EXACT, T>(p, R, src);
+                const T f = eq.source(sp);
+                if (f != T(0)) {
+                    sample += weight * ball_volume<DIM, T>(R) * f * eq.green(R, dist<DIM>(p, sp));
+                }
+            }
+        }
+    }
+    if constexpr (Eq::kScreening) weight *= eq.screening(R);
+    return sphere_step<DIM, EXACT, T>(p, R, walk);
+}
+
+}  // namespace wosb

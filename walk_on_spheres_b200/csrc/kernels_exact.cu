@@ -1,0 +1,277 @@
+// Exact-path kernels: classification, PLAIN_FP64 walks and the FP64
+// closest-point / PRNG checks.  This translation unit is compiled with
+// --fmad=false so double expressions round exactly like the reference's
+// C++17 x86-64 build (no FMA contraction); expression shapes in the device
+// headers follow the reference for the same reason.
+#include <cmath>
+
+#include "kernels.h"
+
+namespace wosb {
+
+namespace {
+
+constexpr int kExactThreads = 128;
+
+__device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000LL); }
+
+// 3D inside test with the reference's ray budget and majority vote
+// (src/inside.cpp:228-260).  Returns the location code; counts retries.
+__device__ int classify_3d(const SceneView &s, const double *p, double bdist, double btol,
+                           int max_ray_attempts, Xoshiro &rng, int &retries) {
+    retries = 0;
+    if (bdist <= btol) return 2;
+    int valid = 0, votes = 0;
+    for (int a = 0; a < max_ray_attempts && valid < 3; ++a) {
+        // random_unit_direction, src/inside.cpp:18-25
+        const double u = rng.unit();
+        const double v = rng.unit();
+        const double z = 2 * u - 1;
+        const double phi = 2 * kPi * v;
+        const double r = sqrt(1 - z * z);
+        const double ray[3] = {r * cos(phi), r * sin(phi), z};
+        bool amb;
+        const int hits = count_ray_hits(s, p, ray, amb);
+        if (amb) {
+            ++retries;
+            continue;
+        }
+        votes += hits & 1;
+        ++valid;
+    }
+    if (valid < 3) return 3;
+    return votes > 1 ? 1 : 0;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kExactThreads)
+    classify_kernel(SceneView s, PointSet ps, uint64_t seed, int max_ray_attempts, double btol,
+                    EqDesc eq, Fields out, uint8_t *location, StartRecord *start,
+                    DeviceCounters *ctr) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < ps.n;
+         t += stride) {
+        double p[3];
+        uint64_t linear;
+        point_at(ps, t, p[0], p[1], p[2], linear);
+        const Nearest<double> q = nearest64<DIM>(s, p[0], p[1], p[2], dinf());
+        StartRecord st;
+        st.radius = sqrt(q.best);
+        st.nx = q.x;
+        st.ny = q.y;
+        st.nz = DIM == 3 ? q.z : 0.0;
+        st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
+        st.pad = 0;
+        int where;
+        if (DIM == 2) {
+            where = st.radius <= btol ? 2 : (winding_number(s, p[0], p[1]) != 0 ? 1 : 0);
+        } else {
+            Xoshiro rng(splitmix64(point_seed(seed, linear) ^ kInsideStream));
+            int retries = 0;
+            where = classify_3d(s, p, st.radius, btol, max_ray_attempts, rng, retries);
+            if (retries) atomicAdd(&ctr->ambiguous_ray_retries, static_cast<unsigned long long>(retries));
+            if (where == 3) atomicAdd(&ctr->indeterminate_points, 1ull);
+        }
+        location[t] = static_cast<uint8_t>(where);
+        start[t] = st;
+        if (out.location) out.location[t] = static_cast<uint8_t>(where);
+        if (where != 1) {
+            double m = __longlong_as_double(0x7ff8000000000000LL), zero = m;
+            if (where == 2) {
+                m = boundary_value<DIM>(eq, V3<double>{st.nx, st.ny, st.nz}, st.boundary_id);
+                zero = 0.0;
+            }
+            if (out.mean) out.mean[t] = m;
+            if (out.variance) out.variance[t] = zero;
+            if (out.standard_error) out.standard_error[t] = zero;
+            if (out.mean_steps) out.mean_steps[t] = zero;
+        }
+    }
+}
+
+template <int DIM, class Eq>
+__global__ void __launch_bounds__(kExactThreads)
+    walk_plain_kernel(SceneView s, PointSet ps, uint64_t seed, Eq eq, int n_walks, double eps,
+                      int max_steps, const uint8_t *__restrict__ location,
+                      const StartRecord *__restrict__ start, Fields out, DeviceCounters *ctr) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < ps.n;
+         t += stride) {
+        if (location[t] != 1) continue;
+        double x, y, z;
+        uint64_t linear;
+        point_at(ps, t, x, y, z, linear);
+        const uint64_t pseed = point_seed(seed, linear);
+        Xoshiro walk(splitmix64(pseed ^ kWalkStream));
+        Xoshiro src(DIM == 2 ? splitmix64(pseed ^ kSourceStream) : 0ull);
+        const StartRecord st = start[t];
+        double mean = 0.0, m2 = 0.0, total_steps = 0.0;
+        unsigned long long steps_sum = 0;
+        int hits = 0;
+        bool overflow = false;
+        for (int i = 0; i < n_walks; ++i) {
+            // wos_sample, include/wos/wos.hpp:54-138
+            V3<double> p{x, y, z};
+            V3<double> np{st.nx, st.ny, st.nz};
+            int bid = st.boundary_id;
+            double R = st.radius;
+            double sample = 0.0, weight = 1.0;
+            int steps = 0;
+            while (R > eps && steps < max_steps) {
+                if (DIM == 2) {
+                    p = walk_body<2, true, double>(eq, p, R, sample, weight, walk, src, overflow);
+                } else {
+                    p = walk_body<3, true, double>(eq, p, R, sample, weight, walk, walk, overflow);
+                }
+                ++steps;
+                const Nearest<double> q = nearest64<DIM>(s, p.x, p.y, p.z, dinf());
+                R = sqrt(q.best);
+                np = V3<double>{q.x, q.y, q.z};
+                if (DIM == 2) bid = s.segid[q.slot].x;
+            }
+            if (R > eps) ++hits;
+            sample += weight * eq.boundary(np, bid);
+            // Welford update, include/wos/wos.hpp:169-180
+            const double count = static_cast<double>(i + 1);
+            const double before = sample - mean;
+            mean += before / count;
+            const double after = sample - mean;
+            m2 += before * after;
+            total_steps += steps;
+            steps_sum += static_cast<unsigned long long>(steps);
+        }
+        const double variance = n_walks > 1 ? m2 / static_cast<double>(n_walks - 1) : 0.0;
+        const double se = n_walks > 0 ? sqrt(variance / static_cast<double>(n_walks)) : 0.0;
+        const double mean_steps = n_walks > 0 ? total_steps / static_cast<double>(n_walks) : 0.0;
+        if (out.mean) out.mean[t] = mean;
+        if (out.variance) out.variance[t] = variance;
+        if (out.standard_error) out.standard_error[t] = se;
+        if (out.mean_steps) out.mean_steps[t] = mean_steps;
+        if (hits) atomicAdd(&ctr->max_steps_hits, static_cast<unsigned long long>(hits));
+        atomicAdd(&ctr->total_steps, steps_sum);
+        atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n_walks));
+        if (overflow) atomicOr(&ctr->error_flags, kErrRejectionCap);
+    }
+}
+
+__global__ void prng_kernel(const uint64_t *seeds, long long n, int count, uint64_t *out) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
+         t += stride) {
+        Xoshiro rng(seeds[t]);
+        for (int i = 0; i < count; ++i) out[t * count + i] = rng.u64();
+    }
+}
+
+template <int DIM>
+__global__ void closest64_kernel(SceneView s, const double *pts, long long n, double *dist,
+                                 double *nearest, int *bid) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
+         t += stride) {
+        const double px = pts[DIM * t], py = pts[DIM * t + 1];
+        const double pz = DIM == 3 ? pts[DIM * t + 2] : 0.0;
+        const Nearest<double> q = nearest64<DIM>(s, px, py, pz, dinf());
+        dist[t] = sqrt(q.best);
+        nearest[DIM * t] = q.x;
+        nearest[DIM * t + 1] = q.y;
+        if (DIM == 3) nearest[DIM * t + 2] = q.z;
+        if (bid) bid[t] = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
+    }
+}
+
+int blocks_for(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > (1ll << 30)) b = 1ll << 30;
+    return static_cast<int>(b);
+}
+
+template <int DIM, class Eq>
+void launch_plain_typed(const SceneView &s, const PointSet &ps, uint64_t seed, const Eq &eq,
+                        int n_walks, double eps, int max_steps, const uint8_t *location,
+                        const StartRecord *start, Fields out, DeviceCounters *ctr,
+                        cudaStream_t stream) {
+    walk_plain_kernel<DIM, Eq><<<blocks_for(ps.n, kExactThreads), kExactThreads, 0, stream>>>(
+        s, ps, seed, eq, n_walks, eps, max_steps, location, start, out, ctr);
+}
+
+template <int DIM>
+void launch_plain_dim(const SceneView &s, const PointSet &ps, uint64_t seed, EqDesc e,
+                      int n_walks, double eps, int max_steps, const uint8_t *location,
+                      const StartRecord *start, Fields out, DeviceCounters *ctr,
+                      cudaStream_t stream) {
+    switch (e.kind) {
+        case kLaplace:
+            launch_plain_typed<DIM>(s, ps, seed, Laplace<DIM>{}, n_walks, eps, max_steps,
+                                    location, start, out, ctr, stream);
+            break;
+        case kPoisson:
+            launch_plain_typed<DIM>(s, ps, seed, Poisson<DIM>{e.mode, e.alpha}, n_walks, eps,
+                                    max_steps, location, start, out, ctr, stream);
+            break;
+        case kScreened:
+            launch_plain_typed<DIM>(s, ps, seed, Screened<DIM>{e.mode, e.alpha}, n_walks, eps,
+                                    max_steps, location, start, out, ctr, stream);
+            break;
+        default:
+            launch_plain_typed<DIM>(s, ps, seed, Helmholtz<DIM>{}, n_walks, eps, max_steps,
+                                    location, start, out, ctr, stream);
+            break;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_classify(const SceneView &s, const PointSet &ps, uint64_t seed,
+                            int max_ray_attempts, double btol, EqDesc eq, Fields out,
+                            uint8_t *location, StartRecord *start, DeviceCounters *counters,
+                            cudaStream_t stream) {
+    if (ps.n <= 0) return cudaSuccess;
+    const int blocks = blocks_for(ps.n, kExactThreads);
+    if (s.dim == 2) {
+        classify_kernel<2><<<blocks, kExactThreads, 0, stream>>>(s, ps, seed, max_ray_attempts,
+                                                                 btol, eq, out, location, start,
+                                                                 counters);
+    } else {
+        classify_kernel<3><<<blocks, kExactThreads, 0, stream>>>(s, ps, seed, max_ray_attempts,
+                                                                 btol, eq, out, location, start,
+                                                                 counters);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_plain(const SceneView &s, const PointSet &ps, uint64_t seed, EqDesc eq,
+                              int n_walks, double eps, int max_steps, const uint8_t *location,
+                              const StartRecord *start, Fields out, DeviceCounters *counters,
+                              cudaStream_t stream) {
+    if (ps.n <= 0) return cudaSuccess;
+    if (s.dim == 2) {
+        launch_plain_dim<2>(s, ps, seed, eq, n_walks, eps, max_steps, location, start, out,
+                            counters, stream);
+    } else {
+        launch_plain_dim<3>(s, ps, seed, eq, n_walks, eps, max_steps, location, start, out,
+                            counters, stream);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prng(const uint64_t *seeds, long long n, int count, uint64_t *out,
+                        cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    prng_kernel<<<blocks_for(n, 128), 128, 0, stream>>>(seeds, n, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closest64(const SceneView &s, const double *pts, long long n, double *dist,
+                             double *nearest, int *bid, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    if (s.dim == 2) {
+        closest64_kernel<2><<<blocks_for(n, 128), 128, 0, stream>>>(s, pts, n, dist, nearest, bid);
+    } else {
+        closest64_kernel<3><<<blocks_for(n, 128), 128, 0, stream>>>(s, pts, n, dist, nearest, bid);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace wosb

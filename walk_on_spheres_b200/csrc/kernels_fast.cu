@@ -1,0 +1,416 @@
+// Fast-path kernels: FAST_FP32 / FAST_FP64 walks and the per-point merge.
+//
+// Scheduling.  A persistent grid of warps pulls tasks from a device queue
+// (one atomicAdd per task).  A task is a chunk of consecutive walks of one
+// grid point; its 32 lanes each run one walk at a time and, when a walk
+// ends, the lane is regenerated with the next walk index of the chunk
+// (warp ballot + popcount rank), so a warp stays full until the chunk's last
+// walks.  Every walk of point p with index w draws from its own Philox
+// stream keyed by p's reference seed, so results do not depend on which
+// lane or warp runs the walk.
+//
+// Precision (FAST_FP32).  Positions, radii, closest-point queries and the
+// sphere step are FP32 against the FP32 scene (staged in shared memory when
+// it fits).  When the FP32 radius falls within `shell_delta` of epsilon the
+// walk re-projects in FP64: an exact FP64 query at the (exactly widened)
+// position decides termination and supplies the nearest point and
+// boundary id for the boundary value, evaluated in FP64.  Per-walk values are
+// accumulated in FP64 (Welford per lane, Chan's merge across lanes and
+// chunks).  FAST_FP64 runs the same scheduling with FP64 everywhere.
+#include <cmath>
+#include <type_traits>
+
+#include "kernels.h"
+
+namespace wosb {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+struct FastRng {
+    PhiloxStream s;
+    __device__ FastRng(uint64_t pseed, uint32_t walk) : s(pseed, walk) {}
+    __device__ __forceinline__ T unit();
+    __device__ __forceinline__ T unit_open() { return unit(); }
+};
+template <>
+__device__ __forceinline__ float FastRng<float>::unit() { return s.uniform_f(); }
+template <>
+__device__ __forceinline__ double FastRng<double>::unit() { return s.uniform_d(); }
+
+struct FastArgs {
+    SceneView s;
+    PointSet ps;
+    uint64_t seed;
+    int n_walks;
+    double eps;
+    int max_steps;
+    double shell_delta;
+    int chunk;
+    int chunks;
+    long long n_tasks;
+    int stage;
+    int pair_f4;   // float4 count of the pair array (staged)
+    int prim_f4;   // float4 count of the primitive array (staged)
+    const uint8_t *location;
+    const StartRecord *start;
+    TaskPartial *partials;
+    unsigned long long *queue;
+    DeviceCounters *ctr;
+};
+
+__device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000LL); }
+
+// Chan et al. pairwise combination of (n, mean, M2).
+__device__ __forceinline__ void chan_merge(double &n, double &mean, double &m2, double nb,
+                                           double meanb, double m2b) {
+    if (nb == 0.0) return;
+    if (n == 0.0) {
+        n = nb;
+        mean = meanb;
+        m2 = m2b;
+        return;
+    }
+    const double tot = n + nb;
+    const double delta = meanb - mean;
+    mean += delta * (nb / tot);
+    m2 += m2b + delta * delta * (n * nb / tot);
+    n = tot;
+}
+
+template <int DIM>
+__device__ __forceinline__ int bid_of(const SceneView &s, int slot) {
+    return (DIM == 2 && slot >= 0) ? s.segid[slot].x : -1;
+}
+
+template <int DIM, class Eq, typename T>
+__global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
+    extern __shared__ float4 smem[];
+    const float4 *pairs = a.s.pair32;
+    const float4 *prims = DIM == 2 ? a.s.seg32 : a.s.tri32;
+    if (std::is_same<T, float>::value && a.stage) {
+        for (int i = threadIdx.x; i < a.pair_f4; i += blockDim.x) smem[i] = pairs[i];
+        for (int i = threadIdx.x; i < a.prim_f4; i += blockDim.x) smem[a.pair_f4 + i] = prims[i];
+        __syncthreads();
+        pairs = smem;
+        prims = smem + a.pair_f4;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const double eps = a.eps;
+    const T eps_hi = static_cast<T>(a.eps + a.shell_delta);
+    const T delta = static_cast<T>(a.shell_delta);
+
+    for (;;) {
+        unsigned long long task = 0;
+        if (lane == 0) task = atomicAdd(a.queue, 1ull);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= static_cast<unsigned long long>(a.n_tasks)) break;
+        const long long pidx = static_cast<long long>(task / a.chunks);
+        const int c = static_cast<int>(task % a.chunks);
+        if (a.location[pidx] != 1) continue;
+
+        double x0, y0, z0;
+        uint64_t linear;
+        point_at(a.ps, pidx, x0, y0, z0, linear);
+        const uint64_t pseed = point_seed(a.seed, linear);
+        const StartRecord st = a.start[pidx];
+        const int w0 = c * a.chunk;
+        const int w1 = min(a.n_walks, w0 + a.chunk);
+
+        // per-lane statistics
+        double n_acc = 0.0, mean_acc = 0.0, m2_acc = 0.0, steps_acc = 0.0;
+        unsigned hits = 0;
+        bool overflow = false;
+
+        // per-lane walk state
+        int walk = w0 + lane;
+        bool active = walk < w1;
+        int next = w0 + 32;
+        V3<T> p{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
+        T R = static_cast<T>(st.radius);
+        T sample = T(0), weight = T(1);
+        int steps = 0;
+        V3<double> np64{st.nx, st.ny, st.nz};  // FAST_FP64: nearest point of the last query
+        int bid64 = st.boundary_id;
+        FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
+
+        while (__any_sync(kFull, active)) {
+            bool done = false;
+            double value = 0.0;
+            if (active) {
+                bool stop = false;
+                V3<double> np{st.nx, st.ny, st.nz};
+                int bid = st.boundary_id;
+                if (steps == 0) {
+                    stop = !(st.radius > eps);  // start point inside the shell
+                } else if (std::is_same<T, double>::value) {
+                    stop = !(static_cast<double>(R) > eps);
+                    np = np64;
+                    bid = bid64;
+                } else if (R <= eps_hi) {
+                    // FP64 re-projection inside the epsilon shell
+                    const double px = p.x, py = p.y, pz = p.z;
+                    const double bound = static_cast<double>(R) + 2.0 * static_cast<double>(delta);
+                    Nearest<double> q = nearest64<DIM>(a.s, px, py, pz, bound * bound);
+                    if (q.slot < 0) q = nearest64<DIM>(a.s, px, py, pz, dinf());
+                    const double r64 = sqrt(q.best);
+                    np = V3<double>{q.x, q.y, q.z};
+                    bid = bid_of<DIM>(a.s, q.slot);
+                    if (r64 <= eps) {
+                        stop = true;
+                    } else {
+                        R = static_cast<T>(r64);
+                    }
+                }
+                if (!stop && steps >= a.max_steps) {
+                    // step cap: finish by projecting to the nearest boundary point
+                    // (include/wos/wos.hpp:129-137)
+                    ++hits;
+                    stop = true;
+                    if (!std::is_same<T, double>::value) {
+                        const Nearest<double> q = nearest64<DIM>(a.s, static_cast<double>(p.x),
+                                                                 static_cast<double>(p.y),
+                                                                 static_cast<double>(p.z), dinf());
+                        np = V3<double>{q.x, q.y, q.z};
+                        bid = bid_of<DIM>(a.s, q.slot);
+                    }
+                }
+                if (stop) {
+                    value = static_cast<double>(sample) +
+                            static_cast<double>(weight) * eq.boundary(np, bid);
+                    done = true;
+                } else {
+                    p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
+                    ++steps;
+                    if (std::is_same<T, float>::value) {
+                        const Nearest<float> q =
+                            nearest32<DIM>(pairs, prims, a.s.n_prims, a.s.depth,
+                                           static_cast<float>(p.x), static_cast<float>(p.y),
+                                           static_cast<float>(p.z), INFINITY);
+                        R = static_cast<T>(sqrtf(q.best));
+                    } else {
+                        const Nearest<double> q = nearest64<DIM>(
+                            a.s, static_cast<double>(p.x), static_cast<double>(p.y),
+                            static_cast<double>(p.z), dinf());
+                        R = static_cast<T>(sqrt(q.best));
+                        np64 = V3<double>{q.x, q.y, q.z};
+                        bid64 = bid_of<DIM>(a.s, q.slot);
+                    }
+                }
+            }
+            if (done) {
+                // Welford update of this lane's statistics
+                n_acc += 1.0;
+                const double before = value - mean_acc;
+                mean_acc += before / n_acc;
+                m2_acc += before * (value - mean_acc);
+                steps_acc += static_cast<double>(steps);
+            }
+            const unsigned done_mask = __ballot_sync(kFull, done);
+            if (done_mask) {
+                if (done) {
+                    walk = next + __popc(done_mask & lt_mask);
+                    active = walk < w1;
+                    if (active) {
+                        p = V3<T>{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
+                        R = static_cast<T>(st.radius);
+                        sample = T(0);
+                        weight = T(1);
+                        steps = 0;
+                        rng = FastRng<T>(pseed, static_cast<uint32_t>(walk));
+                    }
+                }
+                next += __popc(done_mask);
+            }
+        }
+
+        // warp merge of the lanes' statistics
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double nb = __shfl_down_sync(kFull, n_acc, o);
+            const double mb = __shfl_down_sync(kFull, mean_acc, o);
+            const double m2b = __shfl_down_sync(kFull, m2_acc, o);
+            const double sb = __shfl_down_sync(kFull, steps_acc, o);
+            const unsigned hb = __shfl_down_sync(kFull, hits, o);
+            chan_merge(n_acc, mean_acc, m2_acc, nb, mb, m2b);
+            steps_acc += sb;
+            hits += hb;
+        }
+        const unsigned any_overflow = __ballot_sync(kFull, overflow);
+        if (lane == 0) {
+            TaskPartial tp;
+            tp.n = n_acc;
+            tp.mean = mean_acc;
+            tp.m2 = m2_acc;
+            tp.steps = steps_acc;
+            tp.hits = hits;
+            tp.pad = 0;
+            a.partials[task] = tp;
+            if (any_overflow) atomicOr(&a.ctr->error_flags, kErrRejectionCap);
+        }
+    }
+}
+
+// Per-point merge of the chunk statistics (include/wos/wos.hpp:182-190).
+__global__ void merge_kernel(long long n_points, int chunks, int n_walks,
+                             const uint8_t *__restrict__ location,
+                             const TaskPartial *__restrict__ partials, Fields out,
+                             DeviceCounters *ctr) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+         p < n_points; p += stride) {
+        if (location[p] != 1) continue;
+        double n = 0.0, mean = 0.0, m2 = 0.0, steps = 0.0;
+        unsigned long long hits = 0;
+        for (int c = 0; c < chunks; ++c) {
+            const TaskPartial tp = partials[p * chunks + c];
+            chan_merge(n, mean, m2, tp.n, tp.mean, tp.m2);
+            steps += tp.steps;
+            hits += tp.hits;
+        }
+        const double variance = n_walks > 1 ? m2 / static_cast<double>(n_walks - 1) : 0.0;
+        if (out.mean) out.mean[p] = mean;
+        if (out.variance) out.variance[p] = variance;
+        if (out.standard_error) out.standard_error[p] = sqrt(variance / static_cast<double>(n_walks));
+        if (out.mean_steps) out.mean_steps[p] = steps / static_cast<double>(n_walks);
+        if (hits) atomicAdd(&ctr->max_steps_hits, hits);
+        atomicAdd(&ctr->total_steps, static_cast<unsigned long long>(steps));
+        atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n));
+    }
+}
+
+template <int DIM, typename T>
+__global__ void closest32_kernel(SceneView s, const double *pts, long long n, double *dist,
+                                 double *nearest, int *bid) {
+    const float4 *pairs = s.pair32;
+    const float4 *prims = DIM == 2 ? s.seg32 : s.tri32;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
+         t += stride) {
+        const float px = static_cast<float>(pts[DIM * t]);
+        const float py = static_cast<float>(pts[DIM * t + 1]);
+        const float pz = DIM == 3 ? static_cast<float>(pts[DIM * t + 2]) : 0.0f;
+        const Nearest<float> q = nearest32<DIM>(pairs, prims, s.n_prims, s.depth, px, py, pz,
+                                                INFINITY);
+        dist[t] = sqrtf(q.best);
+        nearest[DIM * t] = q.x;
+        nearest[DIM * t + 1] = q.y;
+        if (DIM == 3) nearest[DIM * t + 2] = q.z;
+        if (bid) bid[t] = bid_of<DIM>(s, q.slot);
+    }
+}
+
+template <int DIM, class Eq>
+cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
+                              const FastPlan &plan, cudaStream_t stream) {
+    if (precision == 32) {
+        auto k = walk_fast_kernel<DIM, Eq, float>;
+        if (plan.smem_bytes > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 plan.smem_bytes);
+            if (e != cudaSuccess) return e;
+        }
+        k<<<plan.blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq);
+    } else {
+        walk_fast_kernel<DIM, Eq, double><<<plan.blocks, plan.threads, 0, stream>>>(a, eq);
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM>
+cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const FastPlan &plan,
+                            cudaStream_t stream) {
+    switch (e.kind) {
+        case kLaplace:
+            return launch_fast_typed<DIM>(a, Laplace<DIM>{}, precision, plan, stream);
+        case kPoisson:
+            return launch_fast_typed<DIM>(a, Poisson<DIM>{e.mode, e.alpha}, precision, plan,
+                                          stream);
+        case kScreened:
+            return launch_fast_typed<DIM>(a, Screened<DIM>{e.mode, e.alpha}, precision, plan,
+                                          stream);
+        default:
+            return launch_fast_typed<DIM>(a, Helmholtz<DIM>{}, precision, plan, stream);
+    }
+}
+
+}  // namespace
+
+FastPlan plan_fast(const SceneView &s, long long n_points, int n_walks, int precision,
+                   int device_sms, size_t smem_optin) {
+    FastPlan p{};
+    p.threads = 256;
+    p.chunk = n_walks < 1024 ? n_walks : 1024;
+    if (p.chunk < 1) p.chunk = 1;
+    p.chunks = (n_walks + p.chunk - 1) / p.chunk;
+    p.n_tasks = n_points * p.chunks;
+    const int pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
+    const int prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
+    const size_t bytes = static_cast<size_t>(pair_f4 + prim_f4) * sizeof(float4);
+    p.stage_scene = precision == 32 && bytes <= 96 * 1024 && bytes <= smem_optin;
+    p.smem_bytes = p.stage_scene ? static_cast<int>(bytes) : 0;
+    const int per_sm = precision == 32 ? 4 : 2;
+    p.blocks = device_sms * per_sm;
+    return p;
+}
+
+cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t seed, EqDesc eq,
+                             int n_walks, double epsilon, int max_steps, double shell_delta,
+                             int precision, const FastPlan &plan, const uint8_t *location,
+                             const StartRecord *start, TaskPartial *partials,
+                             unsigned long long *queue, Fields out, DeviceCounters *counters,
+                             cudaStream_t stream, cudaEvent_t after_walk) {
+    if (ps.n <= 0) return cudaSuccess;
+    FastArgs a{};
+    a.s = s;
+    a.ps = ps;
+    a.seed = seed;
+    a.n_walks = n_walks;
+    a.eps = epsilon;
+    a.max_steps = max_steps;
+    a.shell_delta = shell_delta;
+    a.chunk = plan.chunk;
+    a.chunks = plan.chunks;
+    a.n_tasks = plan.n_tasks;
+    a.stage = plan.stage_scene ? 1 : 0;
+    a.pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
+    a.prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
+    a.location = location;
+    a.start = start;
+    a.partials = partials;
+    a.queue = queue;
+    a.ctr = counters;
+    cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    e = s.dim == 2 ? launch_fast_dim<2>(a, eq, precision, plan, stream)
+                   : launch_fast_dim<3>(a, eq, precision, plan, stream);
+    if (e != cudaSuccess) return e;
+    if (after_walk) {
+        e = cudaEventRecord(after_walk, stream);
+        if (e != cudaSuccess) return e;
+    }
+    long long b = (ps.n + 255) / 256;
+    if (b < 1) b = 1;
+    merge_kernel<<<static_cast<int>(b), 256, 0, stream>>>(ps.n, plan.chunks, n_walks, location,
+                                                        partials, out, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closest32(const SceneView &s, const double *pts, long long n, double *dist,
+                             double *nearest, int *bid, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    long long b = (n + 127) / 128;
+    if (s.dim == 2) {
+        closest32_kernel<2, float><<<static_cast<int>(b), 128, 0, stream>>>(s, pts, n, dist,
+                                                                           nearest, bid);
+    } else {
+        closest32_kernel<3, float><<<static_cast<int>(b), 128, 0, stream>>>(s, pts, n, dist,
+                                                                           nearest, bid);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace wosb

@@ -1,0 +1,272 @@
+// Host construction of the device scene: mesh validation, the implicit
+// median-split BVH and the FP64 / FP32 primitive records.
+#include "scene_build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace wosb {
+
+namespace {
+
+struct Item {
+    double lo[3], hi[3], c[3];
+    int prim;
+};
+
+float round_down(double v) {
+    float f = static_cast<float>(v);
+    if (static_cast<double>(f) > v) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+float round_up(double v) {
+    float f = static_cast<float>(v);
+    if (static_cast<double>(f) < v) f = std::nextafter(f, INFINITY);
+    return f;
+}
+
+int first_slot(long long k, long long n, int level) {
+    return static_cast<int>((static_cast<unsigned long long>(k) * static_cast<unsigned long long>(n)) >>
+                            level);
+}
+
+struct Builder {
+    HostScene &sc;
+    std::vector<Item> items;
+
+    void box_of(int s, int e, double *lo, double *hi) const {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = items[s].lo[k];
+            hi[k] = items[s].hi[k];
+        }
+        for (int i = s + 1; i < e; ++i) {
+            for (int k = 0; k < sc.dim; ++k) {
+                lo[k] = lo[k] < items[i].lo[k] ? lo[k] : items[i].lo[k];
+                hi[k] = hi[k] > items[i].hi[k] ? hi[k] : items[i].hi[k];
+            }
+        }
+    }
+
+    // Node `id` (1-based heap index) at `level` covers slots [s, e).
+    void build(long long id, int level, int s, int e) {
+        double lo[3], hi[3];
+        box_of(s, e, lo, hi);
+        const int d = sc.dim;
+        double *b = sc.box64.data() + static_cast<size_t>(2 * d) * id;
+        for (int k = 0; k < d; ++k) {
+            b[k] = lo[k];
+            b[d + k] = hi[k];
+        }
+        if (level == sc.depth) {
+            // leaf: canonical order by primitive id
+            std::sort(items.begin() + s, items.begin() + e,
+                      [](const Item &x, const Item &y) { return x.prim < y.prim; });
+            return;
+        }
+        // longest axis of the node box, ties to the lower axis (src/bvh.cpp:218-224)
+        const double ex = hi[0] - lo[0], ey = hi[1] - lo[1];
+        int axis;
+        if (d == 2) {
+            axis = ex >= ey ? 0 : 1;
+        } else {
+            const double ez = hi[2] - lo[2];
+            axis = (ex >= ey) ? (ex >= ez ? 0 : 2) : (ey >= ez ? 1 : 2);
+        }
+        const long long k = id - (1ll << level);
+        const int mid = first_slot(2 * k + 1, sc.n_prims, level + 1);
+        // median split by (centroid coordinate, primitive id), src/bvh.cpp:143-171
+        std::nth_element(items.begin() + s, items.begin() + mid, items.begin() + e,
+                         [axis](const Item &x, const Item &y) {
+                             if (x.c[axis] < y.c[axis]) return true;
+                             if (x.c[axis] > y.c[axis]) return false;
+                             return x.prim < y.prim;
+                         });
+        build(2 * id, level + 1, s, mid);
+        build(2 * id + 1, level + 1, mid, e);
+    }
+};
+
+}  // namespace
+
+std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                        const int *boundary_ids, int leaf_size, HostScene &sc) {
+    if (dim != 2 && dim != 3) return "mesh dimension must be 2 or 3";
+    if (!verts || n_verts <= 0) return "mesh contains no vertices";
+    if (!prims || n_prims <= 0) {
+        return dim == 2 ? "mesh contains no line primitives" : "mesh contains no triangle primitives";
+    }
+    if (leaf_size == 0) leaf_size = 4;
+    if (leaf_size < 2 || leaf_size > 8) return "leaf_size must be 0 or in [2, 8]";
+    for (long long i = 0; i < static_cast<long long>(n_verts) * dim; ++i) {
+        if (!std::isfinite(verts[i])) return "vertex coordinates must be finite";
+    }
+    for (long long i = 0; i < static_cast<long long>(n_prims) * dim; ++i) {
+        if (prims[i] < 0 || prims[i] >= n_verts) return "primitive vertex index out of range";
+    }
+
+    sc = HostScene{};
+    sc.dim = dim;
+    sc.n_prims = n_prims;
+    sc.n_verts = n_verts;
+    sc.leaf_size = leaf_size;
+    sc.verts.assign(verts, verts + static_cast<size_t>(n_verts) * dim);
+    sc.prims.assign(prims, prims + static_cast<size_t>(n_prims) * dim);
+    sc.boundary_ids.assign(n_prims, 0);
+    if (dim == 2 && boundary_ids) sc.boundary_ids.assign(boundary_ids, boundary_ids + n_prims);
+
+    auto V = [&](int v, int k) { return verts[static_cast<size_t>(dim) * v + k]; };
+
+    // mesh bounding box, src/mesh.cpp:297-322
+    for (int k = 0; k < 3; ++k) {
+        sc.bbox[2 * k] = k < dim ? V(0, k) : 0.0;
+        sc.bbox[2 * k + 1] = sc.bbox[2 * k];
+    }
+    for (int v = 1; v < n_verts; ++v) {
+        for (int k = 0; k < dim; ++k) {
+            const double x = V(v, k);
+            if (x < sc.bbox[2 * k]) sc.bbox[2 * k] = x;
+            else if (x > sc.bbox[2 * k + 1]) sc.bbox[2 * k + 1] = x;
+        }
+    }
+    sc.scale = std::max({1.0, sc.bbox[1] - sc.bbox[0], sc.bbox[3] - sc.bbox[2],
+                         sc.bbox[5] - sc.bbox[4]});
+
+    // primitive boxes and centroids (src/mesh.cpp:324-366); degeneracy checks
+    // (src/mesh.cpp:239-267)
+    Builder B{sc, std::vector<Item>(n_prims)};
+    for (int p = 0; p < n_prims; ++p) {
+        Item &it = B.items[p];
+        std::memset(&it, 0, sizeof(it));
+        it.prim = p;
+        if (dim == 2) {
+            const int a = prims[2 * p], b = prims[2 * p + 1];
+            const double dx = V(b, 0) - V(a, 0), dy = V(b, 1) - V(a, 1);
+            if (!(dx * dx + dy * dy > 0.0)) return "mesh contains a zero-length line segment";
+            for (int k = 0; k < 2; ++k) {
+                it.lo[k] = std::fmin(V(a, k), V(b, k));
+                it.hi[k] = std::fmax(V(a, k), V(b, k));
+                it.c[k] = (V(a, k) + V(b, k)) / 2.0;
+            }
+        } else {
+            const int a = prims[3 * p], b = prims[3 * p + 1], c = prims[3 * p + 2];
+            const double abx = V(b, 0) - V(a, 0), aby = V(b, 1) - V(a, 1), abz = V(b, 2) - V(a, 2);
+            const double acx = V(c, 0) - V(a, 0), acy = V(c, 1) - V(a, 1), acz = V(c, 2) - V(a, 2);
+            const double cx = aby * acz - abz * acy, cy = abz * acx - abx * acz,
+                         cz = abx * acy - aby * acx;
+            if (!(cx * cx + cy * cy + cz * cz > 0.0)) return "mesh contains a degenerate triangle";
+            for (int k = 0; k < 3; ++k) {
+                it.lo[k] = std::fmin(std::fmin(V(a, k), V(b, k)), V(c, k));
+                it.hi[k] = std::fmax(std::fmax(V(a, k), V(b, k)), V(c, k));
+                it.c[k] = (V(a, k) + V(b, k) + V(c, k)) / 3.0;
+            }
+        }
+    }
+
+    // depth: the smallest D with ceil(n / 2^D) <= leaf_size
+    int D = 0;
+    while (((static_cast<long long>(n_prims) + (1ll << D) - 1) >> D) > leaf_size) ++D;
+    if (D > 30) return "mesh too large for the BVH layout";
+    sc.depth = D;
+    const long long n_nodes = 1ll << (D + 1);
+    sc.box64.assign(static_cast<size_t>(n_nodes) * 2 * dim, 0.0);
+    B.build(1, 0, 0, n_prims);
+
+    sc.order.resize(n_prims);
+    for (int s = 0; s < n_prims; ++s) sc.order[s] = B.items[s].prim;
+
+    // FP32 child-pair boxes: outward-rounded FP64 boxes widened by 2^-20 * scale
+    const double widen = std::ldexp(sc.scale, -20);
+    const int rec = dim == 2 ? 8 : 12;
+    const long long n_pairs = 1ll << D;  // parents 1 .. 2^D - 1 (record 0 unused)
+    sc.pair32.assign(static_cast<size_t>(std::max<long long>(n_pairs, 1)) * rec, 0.0f);
+    for (long long i = 1; i < n_pairs; ++i) {
+        float *r = sc.pair32.data() + static_cast<size_t>(rec) * i;
+        for (int side = 0; side < 2; ++side) {
+            const double *b = sc.box64.data() + static_cast<size_t>(2 * dim) * (2 * i + side);
+            float lo[3], hi[3];
+            for (int k = 0; k < dim; ++k) {
+                lo[k] = round_down(b[k] - widen);
+                hi[k] = round_up(b[dim + k] + widen);
+            }
+            if (dim == 2) {
+                float *o = r + 4 * side;
+                o[0] = lo[0];
+                o[1] = lo[1];
+                o[2] = hi[0];
+                o[3] = hi[1];
+            } else {
+                float *o = r + 6 * side;
+                o[0] = lo[0];
+                o[1] = lo[1];
+                o[2] = lo[2];
+                o[3] = hi[0];
+                o[4] = hi[1];
+                o[5] = hi[2];
+            }
+        }
+    }
+
+    // leaf-slot primitive records
+    if (dim == 2) {
+        sc.seg64.resize(static_cast<size_t>(n_prims) * 4);
+        sc.segid.resize(static_cast<size_t>(n_prims) * 2);
+        sc.seg32.resize(static_cast<size_t>(n_prims) * 4);
+        for (int s = 0; s < n_prims; ++s) {
+            const int p = sc.order[s];
+            const int a = prims[2 * p], b = prims[2 * p + 1];
+            const double g[4] = {V(a, 0), V(a, 1), V(b, 0), V(b, 1)};
+            for (int k = 0; k < 4; ++k) {
+                sc.seg64[4 * s + k] = g[k];
+                sc.seg32[4 * s + k] = static_cast<float>(g[k]);
+            }
+            sc.segid[2 * s] = sc.boundary_ids[p];
+            sc.segid[2 * s + 1] = p;
+        }
+    } else {
+        sc.tri64.resize(static_cast<size_t>(n_prims) * 14);
+        sc.tri32.resize(static_cast<size_t>(n_prims) * 16);
+        for (int s = 0; s < n_prims; ++s) {
+            const int p = sc.order[s];
+            const int a = prims[3 * p], b = prims[3 * p + 1], c = prims[3 * p + 2];
+            // Eberly cache, src/bvh.cpp:204-217
+            const double v0[3] = {V(a, 0), V(a, 1), V(a, 2)};
+            const double e1[3] = {V(b, 0) - V(a, 0), V(b, 1) - V(a, 1), V(b, 2) - V(a, 2)};
+            const double e2[3] = {V(c, 0) - V(a, 0), V(c, 1) - V(a, 1), V(c, 2) - V(a, 2)};
+            const double A = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+            const double Bb = e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2];
+            const double Cc = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+            const double det = A * Cc - Bb * Bb;
+            const double denom = A - 2 * Bb + Cc;
+            const double rec64[14] = {v0[0], v0[1], v0[2], e1[0], e1[1], e1[2], e2[0],
+                                      e2[1], e2[2], A,     Bb,    Cc,    det,   denom};
+            std::memcpy(sc.tri64.data() + 14 * static_cast<size_t>(s), rec64, sizeof(rec64));
+            // FP32 record from the rounded vertex and edges
+            float fv[3], fe1[3], fe2[3];
+            for (int k = 0; k < 3; ++k) {
+                fv[k] = static_cast<float>(v0[k]);
+                fe1[k] = static_cast<float>(e1[k]);
+                fe2[k] = static_cast<float>(e2[k]);
+            }
+            double fa = 0, fb = 0, fc = 0;
+            for (int k = 0; k < 3; ++k) {
+                fa += static_cast<double>(fe1[k]) * fe1[k];
+                fb += static_cast<double>(fe1[k]) * fe2[k];
+                fc += static_cast<double>(fe2[k]) * fe2[k];
+            }
+            const double fdet = fa * fc - fb * fb;
+            const double fden = fa - 2 * fb + fc;
+            float *o = sc.tri32.data() + 16 * static_cast<size_t>(s);
+            o[0] = fv[0]; o[1] = fv[1]; o[2] = fv[2]; o[3] = static_cast<float>(fa);
+            o[4] = fe1[0]; o[5] = fe1[1]; o[6] = fe1[2]; o[7] = static_cast<float>(fb);
+            o[8] = fe2[0]; o[9] = fe2[1]; o[10] = fe2[2]; o[11] = static_cast<float>(fc);
+            o[12] = static_cast<float>(fdet);
+            o[13] = static_cast<float>(fden);
+            o[14] = static_cast<float>(1.0 / fdet);
+            o[15] = static_cast<float>(1.0 / fden);
+        }
+    }
+    return std::string();
+}
+
+}  // namespace wosb

@@ -1,0 +1,37 @@
+// Host construction of the device scene (see device/scene.cuh for the layout).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace wosb {
+
+struct HostScene {
+    int dim = 0;
+    int n_prims = 0;
+    int n_verts = 0;
+    int depth = 0;
+    int leaf_size = 4;
+    double bbox[6] = {0, 0, 0, 0, 0, 0};  // xmin, xmax, ymin, ymax, zmin, zmax
+    double scale = 1.0;                   // max(1, largest bbox extent)
+    std::vector<double> box64;   // (2^(D+1)) * 2*dim
+    std::vector<double> seg64;   // 2D: 4 per slot
+    std::vector<int> segid;      // 2D: {boundary_id, prim} per slot
+    std::vector<double> tri64;   // 3D: 14 per slot
+    std::vector<float> pair32;   // 2^D records of 8 (2D) or 12 (3D) floats
+    std::vector<float> seg32;    // 2D: 4 per slot
+    std::vector<float> tri32;    // 3D: 16 per slot
+    std::vector<int> order;      // leaf slot -> primitive id
+    // the mesh itself (for the adjoint's per-vertex data and the checks)
+    std::vector<double> verts;
+    std::vector<int> prims;
+    std::vector<int> boundary_ids;
+};
+
+// Validates the mesh like src/mesh.cpp:239-267 (no zero-length segment, no
+// degenerate triangle, indices in range) and builds the scene.  Returns an
+// empty string on success, otherwise the error message.
+std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                        const int *boundary_ids, int leaf_size, HostScene &out);
+
+}  // namespace wosb
