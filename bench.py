@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU budget of the baseline sample")
+    ap.add_argument("--walks", type=int, default=N_WALKS,
+                    help="walks per point (profiling of smaller cases; the headline uses 4096)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the device solves only (no matched-SE, e2e or CPU legs)")
     return ap.parse_args()
 
 
@@ -195,19 +199,20 @@ def reference_rate(budget_s: float, threads: int | None = None):
             walks += r.counters["inside_points"] * N_WALKS
             secs += r.counters["seconds"]
             ins = r.location[points] == 1
-            var.append(np.nanmean(r.variance[points][ins]))
-        return walks, secs, float(np.mean(var))
+            if ins.any():
+                var.append(float(np.mean(r.variance[points][ins])))
+        return walks, secs, float(np.mean(var)) if var else float("nan")
 
-    # calibrate on a small strided sample, then size the sample to the budget
-    probe = np.arange(0, n_grid, max(1, n_grid // (4 * threads)), dtype=np.int64)
+    # calibrate on a small random sample, then size the sample to the budget
+    order = np.random.default_rng(2024).permutation(n_grid)
+    probe = np.sort(order[:max(8, 2 * threads)])
     w, s, _ = run(probe)
     rate = w / max(s, 1e-9)
-    want_walks = rate * budget_s
-    frac = min(1.0, want_walks / (2 * 0.79 * n_grid * N_WALKS))
-    stride = max(1, int(round(1.0 / max(frac, 1e-9))))
-    pts = np.arange(stride // 2, n_grid, stride, dtype=np.int64)
+    inside_frac = max(w / (len(MODES) * N_WALKS * probe.size), 1e-3)
+    want_points = int(rate * budget_s / (len(MODES) * N_WALKS * inside_frac))
+    pts = np.sort(order[:min(n_grid, max(probe.size, want_points))])
     w, s, var = run(pts)
-    desc = (f"{pts.size} of {n_grid} grid points (stride {stride}), {N_WALKS} walks each, "
+    desc = (f"{pts.size} of {n_grid} grid points (seeded random subset), {N_WALKS} walks each, "
             f"uniform and green source modes")
     return w / s, desc, threads, var
 
@@ -243,7 +248,7 @@ def gpu_arm(args, rank, world, local):
 
     def solve(mode):
         return solver.solve_grid_device("poisson", grid, *[f.data_ptr() for f in fields],
-                                        loc.data_ptr(), N_walks=N_WALKS, epsilon=EPSILON,
+                                        loc.data_ptr(), N_walks=args.walks, epsilon=EPSILON,
                                         seed=seed, source_mode=mode, method=args.method)
 
     for _ in range(args.warmup):
@@ -280,6 +285,16 @@ def gpu_arm(args, rank, world, local):
     else:
         job_s, job_walks = dev_s, float(walks)
     raw_rate = job_walks / job_s
+
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "raw_walks_per_s": raw_rate, "n_gpus": world,
+                              "walks": args.walks, "ms_per_step": job_s * 1000.0 / args.steps,
+                              "walk_kernel_ms": kernel_ms, "clocks": clock}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        solver.close()
+        return
 
     # matched standard error: per-walk variance of the fast path against the
     # FP64 estimator (PLAIN_FP64, the reference's streams) on the same grid

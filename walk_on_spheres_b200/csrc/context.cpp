@@ -78,7 +78,7 @@ wos_context::~wos_context() {
 }
 
 std::vector<DeviceBuffer *> wos_context::all_buffers() {
-    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &tri32, &location, &start,
+    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &location, &start,
             &f_mean, &f_var, &f_se, &f_steps, &f_loc, &partials, &queue, &counters, &points,
             &index, &scratch_a, &scratch_b, &scratch_c, &scratch_d};
 }
@@ -150,6 +150,7 @@ int wos_context::upload_scene() {
     WOS_CUDA(this, upload(tri64, h.tri64, stream), "upload triangles");
     WOS_CUDA(this, upload(pair32, h.pair32, stream), "upload FP32 boxes");
     WOS_CUDA(this, upload(seg32, h.seg32, stream), "upload FP32 segments");
+    WOS_CUDA(this, upload(seg32inv, h.seg32inv, stream), "upload FP32 segment reciprocals");
     WOS_CUDA(this, upload(tri32, h.tri32, stream), "upload FP32 triangles");
     WOS_CUDA(this, cudaStreamSynchronize(stream), "mesh upload");
     view = SceneView{};
@@ -162,6 +163,7 @@ int wos_context::upload_scene() {
     view.tri64 = static_cast<const double2 *>(tri64.ptr);
     view.pair32 = static_cast<const float4 *>(pair32.ptr);
     view.seg32 = static_cast<const float4 *>(seg32.ptr);
+    view.seg32inv = static_cast<const float *>(seg32inv.ptr);
     view.tri32 = static_cast<const float4 *>(tri32.ptr);
     has_mesh = true;
     return WOS_OK;

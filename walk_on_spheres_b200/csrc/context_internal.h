@@ -37,7 +37,7 @@ struct wos_context {
     wosb::SceneView view{};
 
     // scene
-    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, tri32;
+    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32;
     // per solve
     wosb::DeviceBuffer location, start, f_mean, f_var, f_se, f_steps, f_loc, partials, queue,
         counters, points, index;

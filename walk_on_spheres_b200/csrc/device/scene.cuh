@@ -28,9 +28,9 @@
 //          (left, right); 3D 3 float4 packing left lo/hi then right lo/hi.
 //          Boxes are the FP64 boxes rounded outward and widened by 2^-20 of
 //          the mesh scale, so they bound the FP32 primitives.
-//   seg32  2D FP32 segments per slot {x0, y0, x1, y1}
+//   seg32  2D FP32 segments per slot {x0, y0, vx, vy}, seg32inv 1/|v|^2
 //   tri32  3D FP32 Eberly records per slot, 4 float4:
-//          {v0, a} {e1, b} {e2, c} {det, denom, 1/det, 1/denom}
+//          {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}
 #pragma once
 #include <cstdint>
 
@@ -46,6 +46,7 @@ struct SceneView {
     const double2 *tri64;
     const float4 *pair32;  // 2^D pair records (id 0 unused), 2 or 3 float4 each
     const float4 *seg32;
+    const float *seg32inv;  // 2D: 1 / |v|^2 per slot
     const float4 *tri32;
 };
 
@@ -163,14 +164,16 @@ __device__ __forceinline__ double box_dist64(const double *box, const double *p)
 template <typename T>
 struct Nearest {
     T best;      // squared distance (the query's bound until a primitive beats it)
+    T limit;     // nodes are entered only while their box distance is below this
     T x, y, z;   // closest point
     int slot;    // leaf slot of the closest primitive (-1: none beat the bound)
 };
 
 // Stackless near-first traversal.  Policy provides child_dists(id, dl, dr),
-// node_dist(id) and test_leaf(j, Nearest&).
-template <typename T, class Policy>
-__device__ __forceinline__ void traverse_nearest(const Policy &P, int depth, Nearest<T> &q) {
+// node_dist(id) and test_leaf(j, Q&); Q has `limit` (the pruning bound the
+// leaf tests maintain).
+template <typename T, class Policy, class Q>
+__device__ __forceinline__ void traverse_nearest(const Policy &P, int depth, Q &q) {
     if (depth == 0) {
         P.test_leaf(0, q);
         return;
@@ -187,10 +190,10 @@ __device__ __forceinline__ void traverse_nearest(const Policy &P, int depth, Nea
         const T df = left_near ? dr : dl;
         bool descended = false;
         if (cur >= last_internal) {
-            if (dn < q.best) P.test_leaf(static_cast<int>(nearc - leaf_base), q);
-            if (df < q.best) P.test_leaf(static_cast<int>((nearc ^ 1u) - leaf_base), q);
-        } else if (dn < q.best) {
-            bits = (bits << 1) | (df < q.best ? 1u : 0u);
+            if (dn < q.limit) P.test_leaf(static_cast<int>(nearc - leaf_base), q);
+            if (df < q.limit) P.test_leaf(static_cast<int>((nearc ^ 1u) - leaf_base), q);
+        } else if (dn < q.limit) {
+            bits = (bits << 1) | (df < q.limit ? 1u : 0u);
             cur = nearc;
             descended = true;
         }
@@ -198,12 +201,13 @@ __device__ __forceinline__ void traverse_nearest(const Policy &P, int depth, Nea
         // backtrack to the deepest pending far sibling that can still win
         for (;;) {
             if (bits == 0) return;
-            const int tz = __ffs(bits) - 1;
-            bits >>= tz;
-            cur >>= tz;
+            while ((bits & 1u) == 0u) {
+                bits >>= 1;
+                cur >>= 1;
+            }
             bits ^= 1u;
             cur ^= 1u;
-            if (P.node_dist(cur) < q.best) break;
+            if (P.node_dist(cur) < q.limit) break;
         }
     }
 }
@@ -233,6 +237,7 @@ struct Seg64Policy {
             const double d2 = npq_seg64(a.x, a.y, c.x, c.y, p[0], p[1], nx, ny);
             if (d2 < q.best) {
                 q.best = d2;
+                q.limit = d2;
                 q.x = nx;
                 q.y = ny;
                 q.slot = k;
@@ -269,6 +274,7 @@ struct Tri64Policy {
                                              r6.y, nx, ny, nz);
             if (d2 < q.best) {
                 q.best = d2;
+                q.limit = d2;
                 q.x = nx;
                 q.y = ny;
                 q.z = nz;
@@ -285,6 +291,7 @@ __device__ __forceinline__ Nearest<double> nearest64(const SceneView &s, double 
                                                      double pz, double bound2) {
     Nearest<double> q;
     q.best = bound2;
+    q.limit = bound2;
     q.x = q.y = q.z = 0.0;
     q.slot = -1;
     if (DIM == 2) {
@@ -313,9 +320,32 @@ __device__ __forceinline__ float box_dist32_3(float lx, float ly, float lz, floa
     return dx * dx + dy * dy + dz * dz;
 }
 
+// Result of an FP32 query: squared distance, pruning bound and winning slot.
+// Above `exact2` the bound is best * keep with keep = (1 - tau)^2: nodes that
+// could improve the distance by less than a relative tau are skipped, so the
+// true distance d satisfies (1 - tau) sqrt(best) <= d <= sqrt(best) and
+// (1 - tau) sqrt(best) is a radius whose ball lies inside the domain.  Below
+// `exact2` (inside the epsilon shell) pruning is exact.
+struct Nearest32 {
+    float best;
+    float limit;
+    float keep;
+    float exact2;
+    int slot;
+    __device__ __forceinline__ void offer(float d2, int k) {
+        if (d2 < best) {
+            best = d2;
+            slot = k;
+            limit = d2 > exact2 ? d2 * keep : d2;
+        }
+    }
+};
+
+// 2D FP32 segments: {x0, y0, vx, vy} plus 1/|v|^2 per slot.
 struct Seg32Policy {
     const float4 *pairs;
     const float4 *segs;
+    const float *inv;
     int n, depth;
     float px, py;
     __device__ __forceinline__ float node_dist(unsigned id) const {
@@ -325,28 +355,78 @@ struct Seg32Policy {
         dl = box_dist32_2(pairs[2 * id], px, py);
         dr = box_dist32_2(pairs[2 * id + 1], px, py);
     }
-    __device__ __forceinline__ void test_leaf(int j, Nearest<float> &q) const {
+    __device__ __forceinline__ void test_leaf(int j, Nearest32 &q) const {
         const int b = leaf_first(j, n, depth);
         const int e = leaf_first(j + 1, n, depth);
         for (int k = b; k < e; ++k) {
             const float4 g = segs[k];
-            const float vx = g.z - g.x, vy = g.w - g.y;
             const float wx = px - g.x, wy = py - g.y;
-            const float vv = vx * vx + vy * vy;
-            float par = (wx * vx + wy * vy) / vv;
-            par = fminf(fmaxf(par, 0.0f), 1.0f);
-            const float nx = g.x + par * vx, ny = g.y + par * vy;
-            const float dx = px - nx, dy = py - ny;
-            const float d2 = dx * dx + dy * dy;
-            if (d2 < q.best) {
-                q.best = d2;
-                q.x = nx;
-                q.y = ny;
-                q.slot = k;
-            }
+            const float t = fminf(fmaxf((wx * g.z + wy * g.w) * inv[k], 0.0f), 1.0f);
+            const float dx = wx - t * g.z, dy = wy - t * g.w;
+            q.offer(dx * dx + dy * dy, k);
         }
     }
 };
+
+// Eberly's regions in FP32 with precomputed reciprocals; returns the squared
+// distance only.  Record: {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}.
+__device__ __forceinline__ float eberly32(float px, float py, float pz, const float4 *r) {
+    const float4 A = r[0], B = r[1], C = r[2], D = r[3];
+    const float a = A.w, b = B.w, c = C.w, det = D.x;
+    const float bpx = A.x - px, bpy = A.y - py, bpz = A.z - pz;
+    const float d = B.x * bpx + B.y * bpy + B.z * bpz;
+    const float e = C.x * bpx + C.y * bpy + C.z * bpz;
+    float s = b * e - c * d;
+    float t = b * d - a * e;
+    if (s + t <= det) {
+        if (s < 0.0f) {
+            if (t < 0.0f && d < 0.0f) {  // region 4, edge t = 0
+                t = 0.0f;
+                s = (-d >= a) ? 1.0f : -d * D.z;
+            } else {  // regions 3 and 4, edge s = 0
+                s = 0.0f;
+                t = (e >= 0.0f) ? 0.0f : ((-e >= c) ? 1.0f : -e * D.w);
+            }
+        } else if (t < 0.0f) {  // region 5
+            t = 0.0f;
+            s = (d >= 0.0f) ? 0.0f : ((-d >= a) ? 1.0f : -d * D.z);
+        } else {  // region 0
+            s *= D.y;
+            t *= D.y;
+        }
+    } else {
+        const float denom = a - 2.0f * b + c;
+        if (s < 0.0f) {  // region 2
+            const float bd = b + d, ce = c + e;
+            if (ce > bd) {
+                const float numer = ce - bd;
+                s = (numer >= denom) ? 1.0f : __fdividef(numer, denom);
+                t = 1.0f - s;
+            } else {
+                s = 0.0f;
+                t = (ce <= 0.0f) ? 1.0f : ((e >= 0.0f) ? 0.0f : -e * D.w);
+            }
+        } else if (t < 0.0f) {  // region 6
+            const float be = b + e, ad = a + d;
+            if (ad > be) {
+                const float numer = ad - be;
+                t = (numer >= denom) ? 1.0f : __fdividef(numer, denom);
+                s = 1.0f - t;
+            } else {
+                t = 0.0f;
+                s = (ad <= 0.0f) ? 1.0f : ((d >= 0.0f) ? 0.0f : -d * D.z);
+            }
+        } else {  // region 1
+            const float numer = (c + e) - (b + d);
+            s = (numer <= 0.0f) ? 0.0f : ((numer >= denom) ? 1.0f : __fdividef(numer, denom));
+            t = 1.0f - s;
+        }
+    }
+    const float dx = bpx + s * B.x + t * C.x;
+    const float dy = bpy + s * B.y + t * C.y;
+    const float dz = bpz + s * B.z + t * C.z;
+    return dx * dx + dy * dy + dz * dz;
+}
 
 struct Tri32Policy {
     const float4 *pairs;
@@ -368,38 +448,28 @@ struct Tri32Policy {
         dl = box_dist32_3(a.x, a.y, a.z, a.w, b.x, b.y, px, py, pz);
         dr = box_dist32_3(b.z, b.w, c.x, c.y, c.z, c.w, px, py, pz);
     }
-    __device__ __forceinline__ void test_leaf(int j, Nearest<float> &q) const {
+    __device__ __forceinline__ void test_leaf(int j, Nearest32 &q) const {
         const int b = leaf_first(j, n, depth);
         const int e = leaf_first(j + 1, n, depth);
-        for (int k = b; k < e; ++k) {
-            const float4 *r = tris + 4 * k;
-            const float4 A = r[0], B = r[1], Cc = r[2], Dd = r[3];
-            float nx, ny, nz;
-            const float d2 = eberly<float>(px, py, pz, A.x, A.y, A.z, B.x, B.y, B.z, Cc.x, Cc.y,
-                                           Cc.z, A.w, B.w, Cc.w, Dd.x, Dd.y, nx, ny, nz);
-            if (d2 < q.best) {
-                q.best = d2;
-                q.x = nx;
-                q.y = ny;
-                q.z = nz;
-                q.slot = k;
-            }
-        }
+        for (int k = b; k < e; ++k) q.offer(eberly32(px, py, pz, tris + 4 * k), k);
     }
 };
 
-// FP32 closest point through the given pair/primitive arrays (global or
-// shared memory).
+// FP32 closest-point query through the given pair / primitive arrays (global
+// or shared memory), conservative to a relative tolerance tau above the exact
+// radius sqrt(exact2) (see Nearest32).
 template <int DIM>
-__device__ __forceinline__ Nearest<float> nearest32(const float4 *pairs, const float4 *prims,
-                                                    int n, int depth, float px, float py,
-                                                    float pz, float bound2) {
-    Nearest<float> q;
-    q.best = bound2;
-    q.x = q.y = q.z = 0.0f;
+__device__ __forceinline__ Nearest32 nearest32(const float4 *pairs, const float4 *prims,
+                                               const float *inv, int n, int depth, float px,
+                                               float py, float pz, float keep, float exact2) {
+    Nearest32 q;
+    q.best = INFINITY;
+    q.limit = INFINITY;
+    q.keep = keep;
+    q.exact2 = exact2;
     q.slot = -1;
     if (DIM == 2) {
-        Seg32Policy P{pairs, prims, n, depth, px, py};
+        Seg32Policy P{pairs, prims, inv, n, depth, px, py};
         traverse_nearest<float>(P, depth, q);
     } else {
         Tri32Policy P{pairs, prims, n, depth, px, py, pz};

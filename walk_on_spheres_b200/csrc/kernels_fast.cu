@@ -48,12 +48,17 @@ struct FastArgs {
     double eps;
     int max_steps;
     double shell_delta;
+    float keep;     // (1 - tau)^2: approximate pruning bound of the FP32 query
+    float shrink;   // 1 - tau: conservative radius factor
+    float exact2;   // below this squared distance the FP32 query prunes exactly
+    float shell2;   // (eps + shell_delta)^2: FP32 radius inside the epsilon shell
     int chunk;
     int chunks;
     long long n_tasks;
     int stage;
     int pair_f4;   // float4 count of the pair array (staged)
     int prim_f4;   // float4 count of the primitive array (staged)
+    int aux_f4;    // float4 count of the 2D reciprocal array (staged)
     const uint8_t *location;
     const StartRecord *start;
     TaskPartial *partials;
@@ -85,23 +90,51 @@ __device__ __forceinline__ int bid_of(const SceneView &s, int slot) {
     return (DIM == 2 && slot >= 0) ? s.segid[slot].x : -1;
 }
 
+// FP64 re-projection of p onto the primitive in `slot` (the FP32 query's
+// winner): exact distance, nearest point and (2D) boundary id.
+template <int DIM>
+__device__ __forceinline__ double reproject64(const SceneView &s, int slot, double px, double py,
+                                              double pz, V3<double> &np, int &bid) {
+    if (DIM == 2) {
+        const double2 a = s.seg64[2 * slot], c = s.seg64[2 * slot + 1];
+        double nx, ny;
+        const double d2 = npq_seg64(a.x, a.y, c.x, c.y, px, py, nx, ny);
+        np = V3<double>{nx, ny, 0.0};
+        bid = s.segid[slot].x;
+        return sqrt(d2);
+    }
+    const double2 *r = s.tri64 + 7 * slot;
+    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5], r6 = r[6];
+    double nx, ny, nz;
+    const double d2 = eberly<double>(px, py, pz, r0.x, r0.y, r1.x, r1.y, r2.x, r2.y, r3.x, r3.y,
+                                     r4.x, r4.y, r5.x, r5.y, r6.x, r6.y, nx, ny, nz);
+    np = V3<double>{nx, ny, nz};
+    bid = -1;
+    return sqrt(d2);
+}
+
 template <int DIM, class Eq, typename T>
 __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
+    constexpr bool kF32 = std::is_same<T, float>::value;
     extern __shared__ float4 smem[];
     const float4 *pairs = a.s.pair32;
     const float4 *prims = DIM == 2 ? a.s.seg32 : a.s.tri32;
-    if (std::is_same<T, float>::value && a.stage) {
+    const float *inv = a.s.seg32inv;
+    if (kF32 && a.stage) {
         for (int i = threadIdx.x; i < a.pair_f4; i += blockDim.x) smem[i] = pairs[i];
         for (int i = threadIdx.x; i < a.prim_f4; i += blockDim.x) smem[a.pair_f4 + i] = prims[i];
+        float *aux = reinterpret_cast<float *>(smem + a.pair_f4 + a.prim_f4);
+        if (DIM == 2) {
+            for (int i = threadIdx.x; i < a.s.n_prims; i += blockDim.x) aux[i] = inv[i];
+        }
         __syncthreads();
         pairs = smem;
         prims = smem + a.pair_f4;
+        inv = aux;
     }
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const double eps = a.eps;
-    const T eps_hi = static_cast<T>(a.eps + a.shell_delta);
-    const T delta = static_cast<T>(a.shell_delta);
 
     for (;;) {
         unsigned long long task = 0;
@@ -116,12 +149,16 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
         uint64_t linear;
         point_at(a.ps, pidx, x0, y0, z0, linear);
         const uint64_t pseed = point_seed(a.seed, linear);
-        const StartRecord st = a.start[pidx];
+        const V3<T> p0{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
+        const double r0 = a.start[pidx].radius;
+        const T R0 = static_cast<T>(r0);
+        const bool start_stops = !(r0 > eps);  // start point already inside the shell
         const int w0 = c * a.chunk;
         const int w1 = min(a.n_walks, w0 + a.chunk);
 
         // per-lane statistics
-        double n_acc = 0.0, mean_acc = 0.0, m2_acc = 0.0, steps_acc = 0.0;
+        int n_acc = 0, steps_acc = 0;
+        double mean_acc = 0.0, m2_acc = 0.0;
         unsigned hits = 0;
         bool overflow = false;
 
@@ -129,12 +166,13 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
         int walk = w0 + lane;
         bool active = walk < w1;
         int next = w0 + 32;
-        V3<T> p{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
-        T R = static_cast<T>(st.radius);
+        V3<T> p = p0;
+        T R = R0;
         T sample = T(0), weight = T(1);
         int steps = 0;
-        V3<double> np64{st.nx, st.ny, st.nz};  // FAST_FP64: nearest point of the last query
-        int bid64 = st.boundary_id;
+        int slot = -1;                 // FP32: winner of the last query
+        V3<double> np64{0.0, 0.0, 0.0};  // FP64: nearest point of the last query
+        int bid64 = -1;
         FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
 
         while (__any_sync(kFull, active)) {
@@ -142,40 +180,42 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
             double value = 0.0;
             if (active) {
                 bool stop = false;
-                V3<double> np{st.nx, st.ny, st.nz};
-                int bid = st.boundary_id;
+                V3<double> np{0.0, 0.0, 0.0};
+                int bid = -1;
                 if (steps == 0) {
-                    stop = !(st.radius > eps);  // start point inside the shell
-                } else if (std::is_same<T, double>::value) {
+                    stop = start_stops;
+                    if (stop) {
+                        const StartRecord st = a.start[pidx];
+                        np = V3<double>{st.nx, st.ny, st.nz};
+                        bid = st.boundary_id;
+                    }
+                } else if (!kF32) {
                     stop = !(static_cast<double>(R) > eps);
                     np = np64;
                     bid = bid64;
-                } else if (R <= eps_hi) {
-                    // FP64 re-projection inside the epsilon shell
-                    const double px = p.x, py = p.y, pz = p.z;
-                    const double bound = static_cast<double>(R) + 2.0 * static_cast<double>(delta);
-                    Nearest<double> q = nearest64<DIM>(a.s, px, py, pz, bound * bound);
-                    if (q.slot < 0) q = nearest64<DIM>(a.s, px, py, pz, dinf());
-                    const double r64 = sqrt(q.best);
-                    np = V3<double>{q.x, q.y, q.z};
-                    bid = bid_of<DIM>(a.s, q.slot);
-                    if (r64 <= eps) {
+                } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
+                    // epsilon shell: FP64 re-projection onto the nearest primitive
+                    const double d64 = reproject64<DIM>(a.s, slot, static_cast<double>(p.x),
+                                                        static_cast<double>(p.y),
+                                                        static_cast<double>(p.z), np, bid);
+                    if (d64 <= eps) {
                         stop = true;
                     } else {
-                        R = static_cast<T>(r64);
+                        R = static_cast<T>(d64);
                     }
                 }
                 if (!stop && steps >= a.max_steps) {
-                    // step cap: finish by projecting to the nearest boundary point
+                    // step cap: finish at the nearest boundary point
                     // (include/wos/wos.hpp:129-137)
                     ++hits;
                     stop = true;
-                    if (!std::is_same<T, double>::value) {
-                        const Nearest<double> q = nearest64<DIM>(a.s, static_cast<double>(p.x),
-                                                                 static_cast<double>(p.y),
-                                                                 static_cast<double>(p.z), dinf());
-                        np = V3<double>{q.x, q.y, q.z};
-                        bid = bid_of<DIM>(a.s, q.slot);
+                    if (kF32) {
+                        reproject64<DIM>(a.s, slot, static_cast<double>(p.x),
+                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
+                                         bid);
+                    } else {
+                        np = np64;
+                        bid = bid64;
                     }
                 }
                 if (stop) {
@@ -185,12 +225,13 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                 } else {
                     p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
                     ++steps;
-                    if (std::is_same<T, float>::value) {
-                        const Nearest<float> q =
-                            nearest32<DIM>(pairs, prims, a.s.n_prims, a.s.depth,
-                                           static_cast<float>(p.x), static_cast<float>(p.y),
-                                           static_cast<float>(p.z), INFINITY);
-                        R = static_cast<T>(sqrtf(q.best));
+                    if constexpr (kF32) {
+                        const Nearest32 q = nearest32<DIM>(pairs, prims, inv, a.s.n_prims,
+                                                           a.s.depth, p.x, p.y, p.z, a.keep,
+                                                           a.exact2);
+                        const float r = sqrtf(q.best);
+                        R = q.best > a.shell2 ? r * a.shrink : r;
+                        slot = q.slot;
                     } else {
                         const Nearest<double> q = nearest64<DIM>(
                             a.s, static_cast<double>(p.x), static_cast<double>(p.y),
@@ -203,11 +244,11 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
             }
             if (done) {
                 // Welford update of this lane's statistics
-                n_acc += 1.0;
+                ++n_acc;
                 const double before = value - mean_acc;
-                mean_acc += before / n_acc;
+                mean_acc += before / static_cast<double>(n_acc);
                 m2_acc += before * (value - mean_acc);
-                steps_acc += static_cast<double>(steps);
+                steps_acc += steps;
             }
             const unsigned done_mask = __ballot_sync(kFull, done);
             if (done_mask) {
@@ -215,8 +256,8 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                     walk = next + __popc(done_mask & lt_mask);
                     active = walk < w1;
                     if (active) {
-                        p = V3<T>{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
-                        R = static_cast<T>(st.radius);
+                        p = p0;
+                        R = R0;
                         sample = T(0);
                         weight = T(1);
                         steps = 0;
@@ -228,24 +269,26 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
         }
 
         // warp merge of the lanes' statistics
+        double n_tot = static_cast<double>(n_acc);
+        unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            const double nb = __shfl_down_sync(kFull, n_acc, o);
+            const double nb = __shfl_down_sync(kFull, n_tot, o);
             const double mb = __shfl_down_sync(kFull, mean_acc, o);
             const double m2b = __shfl_down_sync(kFull, m2_acc, o);
-            const double sb = __shfl_down_sync(kFull, steps_acc, o);
+            const unsigned long long sb = __shfl_down_sync(kFull, steps_tot, o);
             const unsigned hb = __shfl_down_sync(kFull, hits, o);
-            chan_merge(n_acc, mean_acc, m2_acc, nb, mb, m2b);
-            steps_acc += sb;
+            chan_merge(n_tot, mean_acc, m2_acc, nb, mb, m2b);
+            steps_tot += sb;
             hits += hb;
         }
         const unsigned any_overflow = __ballot_sync(kFull, overflow);
         if (lane == 0) {
             TaskPartial tp;
-            tp.n = n_acc;
+            tp.n = n_tot;
             tp.mean = mean_acc;
             tp.m2 = m2_acc;
-            tp.steps = steps_acc;
+            tp.steps = static_cast<double>(steps_tot);
             tp.hits = hits;
             tp.pad = 0;
             a.partials[task] = tp;
@@ -293,19 +336,42 @@ __global__ void closest32_kernel(SceneView s, const double *pts, long long n, do
         const float px = static_cast<float>(pts[DIM * t]);
         const float py = static_cast<float>(pts[DIM * t + 1]);
         const float pz = DIM == 3 ? static_cast<float>(pts[DIM * t + 2]) : 0.0f;
-        const Nearest<float> q = nearest32<DIM>(pairs, prims, s.n_prims, s.depth, px, py, pz,
-                                                INFINITY);
+        // exact FP32 query (keep = 1), nearest point by FP64 re-projection
+        const Nearest32 q = nearest32<DIM>(pairs, prims, s.seg32inv, s.n_prims, s.depth, px, py,
+                                           pz, 1.0f, 0.0f);
         dist[t] = sqrtf(q.best);
-        nearest[DIM * t] = q.x;
-        nearest[DIM * t + 1] = q.y;
-        if (DIM == 3) nearest[DIM * t + 2] = q.z;
-        if (bid) bid[t] = bid_of<DIM>(s, q.slot);
+        V3<double> np;
+        int b = -1;
+        reproject64<DIM>(s, q.slot, px, py, pz, np, b);
+        nearest[DIM * t] = np.x;
+        nearest[DIM * t + 1] = np.y;
+        if (DIM == 3) nearest[DIM * t + 2] = np.z;
+        if (bid) bid[t] = b;
     }
 }
 
 template <int DIM, class Eq>
 cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
                               const FastPlan &plan, cudaStream_t stream) {
+    // persistent grid: every block that can be resident at once (plan.blocks
+    // overrides when positive)
+    auto grid_for = [&](auto kernel, int smem, int &blocks) -> cudaError_t {
+        if (plan.blocks > 0) {
+            blocks = plan.blocks;
+            return cudaSuccess;
+        }
+        int per_sm = 0, dev = 0, sms = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                                      plan.threads, smem);
+        if (e != cudaSuccess) return e;
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        blocks = sms * (per_sm > 0 ? per_sm : 1);
+        return cudaSuccess;
+    };
+    int blocks = 0;
     if (precision == 32) {
         auto k = walk_fast_kernel<DIM, Eq, float>;
         if (plan.smem_bytes > 48 * 1024) {
@@ -313,9 +379,14 @@ cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
                                                  plan.smem_bytes);
             if (e != cudaSuccess) return e;
         }
-        k<<<plan.blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq);
+        cudaError_t e = grid_for(k, plan.smem_bytes, blocks);
+        if (e != cudaSuccess) return e;
+        k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq);
     } else {
-        walk_fast_kernel<DIM, Eq, double><<<plan.blocks, plan.threads, 0, stream>>>(a, eq);
+        auto k = walk_fast_kernel<DIM, Eq, double>;
+        cudaError_t e = grid_for(k, 0, blocks);
+        if (e != cudaSuccess) return e;
+        k<<<blocks, plan.threads, 0, stream>>>(a, eq);
     }
     return cudaGetLastError();
 }
@@ -349,11 +420,12 @@ FastPlan plan_fast(const SceneView &s, long long n_points, int n_walks, int prec
     p.n_tasks = n_points * p.chunks;
     const int pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
     const int prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
-    const size_t bytes = static_cast<size_t>(pair_f4 + prim_f4) * sizeof(float4);
+    const int aux_f4 = s.dim == 2 ? (s.n_prims + 3) / 4 : 0;
+    const size_t bytes = static_cast<size_t>(pair_f4 + prim_f4 + aux_f4) * sizeof(float4);
     p.stage_scene = precision == 32 && bytes <= 96 * 1024 && bytes <= smem_optin;
     p.smem_bytes = p.stage_scene ? static_cast<int>(bytes) : 0;
-    const int per_sm = precision == 32 ? 4 : 2;
-    p.blocks = device_sms * per_sm;
+    (void)device_sms;
+    p.blocks = 0;  // sized from the occupancy of the chosen kernel at launch
     return p;
 }
 
@@ -378,6 +450,15 @@ cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t se
     a.stage = plan.stage_scene ? 1 : 0;
     a.pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
     a.prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
+    a.aux_f4 = s.dim == 2 ? (s.n_prims + 3) / 4 : 0;
+    // FP32 queries are conservative to a relative tau = 2^-10 outside the
+    // epsilon shell and exact inside it (see Nearest32)
+    const double tau = 1.0 / 1024.0;
+    const double shell = epsilon + shell_delta;
+    a.keep = static_cast<float>((1.0 - tau) * (1.0 - tau));
+    a.shrink = static_cast<float>(1.0 - tau);
+    a.shell2 = static_cast<float>(shell * shell);
+    a.exact2 = static_cast<float>(shell * shell / ((1.0 - tau) * (1.0 - tau)));
     a.location = location;
     a.start = start;
     a.partials = partials;

@@ -212,14 +212,21 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
         sc.seg64.resize(static_cast<size_t>(n_prims) * 4);
         sc.segid.resize(static_cast<size_t>(n_prims) * 2);
         sc.seg32.resize(static_cast<size_t>(n_prims) * 4);
+        sc.seg32inv.resize(static_cast<size_t>(n_prims));
         for (int s = 0; s < n_prims; ++s) {
             const int p = sc.order[s];
             const int a = prims[2 * p], b = prims[2 * p + 1];
             const double g[4] = {V(a, 0), V(a, 1), V(b, 0), V(b, 1)};
-            for (int k = 0; k < 4; ++k) {
-                sc.seg64[4 * s + k] = g[k];
-                sc.seg32[4 * s + k] = static_cast<float>(g[k]);
-            }
+            for (int k = 0; k < 4; ++k) sc.seg64[4 * s + k] = g[k];
+            // FP32: origin, direction and 1/|direction|^2
+            const float x0 = static_cast<float>(g[0]), y0 = static_cast<float>(g[1]);
+            const float vx = static_cast<float>(g[2] - g[0]), vy = static_cast<float>(g[3] - g[1]);
+            sc.seg32[4 * s + 0] = x0;
+            sc.seg32[4 * s + 1] = y0;
+            sc.seg32[4 * s + 2] = vx;
+            sc.seg32[4 * s + 3] = vy;
+            sc.seg32inv[s] = static_cast<float>(
+                1.0 / (static_cast<double>(vx) * vx + static_cast<double>(vy) * vy));
             sc.segid[2 * s] = sc.boundary_ids[p];
             sc.segid[2 * s + 1] = p;
         }
@@ -255,15 +262,14 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
                 fc += static_cast<double>(fe2[k]) * fe2[k];
             }
             const double fdet = fa * fc - fb * fb;
-            const double fden = fa - 2 * fb + fc;
             float *o = sc.tri32.data() + 16 * static_cast<size_t>(s);
             o[0] = fv[0]; o[1] = fv[1]; o[2] = fv[2]; o[3] = static_cast<float>(fa);
             o[4] = fe1[0]; o[5] = fe1[1]; o[6] = fe1[2]; o[7] = static_cast<float>(fb);
             o[8] = fe2[0]; o[9] = fe2[1]; o[10] = fe2[2]; o[11] = static_cast<float>(fc);
             o[12] = static_cast<float>(fdet);
-            o[13] = static_cast<float>(fden);
-            o[14] = static_cast<float>(1.0 / fdet);
-            o[15] = static_cast<float>(1.0 / fden);
+            o[13] = static_cast<float>(1.0 / fdet);
+            o[14] = static_cast<float>(1.0 / fa);
+            o[15] = static_cast<float>(1.0 / fc);
         }
     }
     return std::string();
