@@ -78,7 +78,7 @@ wos_context::~wos_context() {
 }
 
 std::vector<DeviceBuffer *> wos_context::all_buffers() {
-    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &location, &start,
+    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &wbox, &wprim, &wide2bin, &woff, &location, &start,
             &f_mean, &f_var, &f_se, &f_steps, &f_loc, &partials, &queue, &counters, &points,
             &index, &scratch_a, &scratch_b, &scratch_c, &scratch_d};
 }
@@ -152,6 +152,11 @@ int wos_context::upload_scene() {
     WOS_CUDA(this, upload(seg32, h.seg32, stream), "upload FP32 segments");
     WOS_CUDA(this, upload(seg32inv, h.seg32inv, stream), "upload FP32 segment reciprocals");
     WOS_CUDA(this, upload(tri32, h.tri32, stream), "upload FP32 triangles");
+    WOS_CUDA(this, upload(wbox, h.wbox, stream), "upload wide boxes");
+    WOS_CUDA(this, upload(wprim, h.wprim, stream), "upload wide primitives");
+    WOS_CUDA(this, upload(wide2bin, h.wide2bin, stream), "upload wide slot map");
+    WOS_CUDA(this, upload(woff, std::vector<int>(h.w_off, h.w_off + 8), stream),
+             "upload wide offsets");
     WOS_CUDA(this, cudaStreamSynchronize(stream), "mesh upload");
     view = SceneView{};
     view.dim = h.dim;
@@ -165,6 +170,16 @@ int wos_context::upload_scene() {
     view.seg32 = static_cast<const float4 *>(seg32.ptr);
     view.seg32inv = static_cast<const float *>(seg32inv.ptr);
     view.tri32 = static_cast<const float4 *>(tri32.ptr);
+    wide = WideView{};
+    wide.dim = h.dim;
+    wide.H = h.wH;
+    wide.n = h.n_prims;
+    wide.npad = h.w_npad;
+    wide.box_total = h.w_box_total;
+    wide.off = static_cast<const int *>(woff.ptr);
+    wide.box = static_cast<const float *>(wbox.ptr);
+    wide.prim = static_cast<const float *>(wprim.ptr);
+    wide.wide2bin = static_cast<const int *>(wide2bin.ptr);
     has_mesh = true;
     return WOS_OK;
 }
@@ -273,7 +288,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
                  "plain walk kernel");
     } else {
         const int precision = p.method == WOS_METHOD_FAST_FP32 ? 32 : 64;
-        FastPlan plan = plan_fast(view, n, p.N_walks, precision, sms, smem_optin);
+        FastPlan plan = plan_fast(view, wide, n, p.N_walks, precision, sms, smem_optin);
         if (chunk_override > 0) {
             plan.chunk = std::min(chunk_override, p.N_walks);
             plan.chunks = (p.N_walks + plan.chunk - 1) / plan.chunk;
@@ -286,7 +301,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
         // FP32 error margin of the shell test: positions, vertices and the
         // query arithmetic carry ~1e-7 relative error of the mesh scale.
         const double shell_delta = std::ldexp(scene.scale, -16);
-        WOS_CUDA(this, launch_walk_fast(view, ps, p.seed, eq, p.N_walks, eps, p.max_steps,
+        WOS_CUDA(this, launch_walk_fast(view, wide, ps, p.seed, eq, p.N_walks, eps, p.max_steps,
                                         shell_delta, precision, plan, loc, st,
                                         static_cast<TaskPartial *>(partials.ptr),
                                         static_cast<unsigned long long *>(queue.ptr), out, ctr,
@@ -513,7 +528,7 @@ extern "C" int wos_closest_points(wos_context *ctx, int precision, const double 
     auto *dn = static_cast<double *>(ctx->scratch_c.ptr);
     auto *db = static_cast<int *>(ctx->scratch_d.ptr);
     cudaError_t e = precision == 64 ? launch_closest64(ctx->view, dp, n, dd, dn, db, ctx->stream)
-                                    : launch_closest32(ctx->view, dp, n, dd, dn, db, ctx->stream);
+                                    : launch_closest32(ctx->view, ctx->wide, dp, n, dd, dn, db, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "closest-point kernel");
     WOS_CUDA(ctx, cudaMemcpyAsync(dist, dd, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     WOS_CUDA(ctx, cudaMemcpyAsync(nearest, dn, sizeof(double) * dim * n, cudaMemcpyDeviceToHost, ctx->stream), "D2H");

@@ -35,9 +35,11 @@ struct wos_context {
     bool has_mesh = false;
     wosb::HostScene scene;
     wosb::SceneView view{};
+    wosb::WideView wide{};
 
     // scene
-    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32;
+    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
+        wide2bin, woff;
     // per solve
     wosb::DeviceBuffer location, start, f_mean, f_var, f_se, f_steps, f_loc, partials, queue,
         counters, points, index;

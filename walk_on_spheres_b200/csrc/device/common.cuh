@@ -5,6 +5,7 @@
 #include "equations.cuh"
 #include "prng.cuh"
 #include "scene.cuh"
+#include "wide.cuh"
 
 namespace wosb {
 

@@ -36,6 +36,8 @@
 
 namespace wosb {
 
+struct WideView;
+
 struct SceneView {
     int dim;
     int n_prims;

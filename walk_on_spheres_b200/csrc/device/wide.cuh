@@ -1,0 +1,149 @@
+// Warp-cooperative closest-point queries on a 32-wide BVH (FAST_FP32 path).
+//
+// Layout (built by scene_build.cpp): primitives sit in "wide slots" ordered by
+// recursive median bisection; the node at height h with index i covers slots
+// [i * 32^h, (i+1) * 32^h), so the children of node i are nodes 32i .. 32i+31
+// one height below and no pointers are stored.  The root has height H
+// (32^H >= n).  Child boxes of heights 1 .. H-1 and the primitives are stored
+// structure-of-arrays (one float array per coordinate / record field), so lane
+// k of a warp reads child k or slot k with conflict-free, coalesced accesses.
+// Padding boxes are empty (infinitely far) and padding primitives lie at
+// 1e30, so every lane always has something to test.
+//
+// Traversal: one query at a time per warp, all 32 lanes working on it.  At a
+// node every lane computes the box distance of one child; the nearest pending
+// child is found with one redux.sync.min over a key (distance bits with the
+// lane in the low 5 bits); a leaf cluster's 32 primitives are tested in
+// parallel and reduced with redux.sync.min.  It is stackless: the state is
+// (height, node); going back up recomputes the parent's child distances and
+// keeps the children whose key is above the one just left, which are exactly
+// the pending ones because children are taken in increasing key order.
+//
+// Pruning is conservative to a relative tau above the epsilon shell (see
+// Nearest32 in scene.cuh): bound = best * keep while best > exact2.
+#pragma once
+#include <cstdint>
+
+namespace wosb {
+
+struct WideView {
+    int dim;
+    int H;             // root height
+    int n;             // primitives
+    int npad;          // primitive slots (multiple of 32)
+    int box_total;     // entries per box coordinate array
+    const int *off;    // [8]: offset of height h in each box coordinate array
+    const float *box;  // 2*dim arrays of box_total floats
+    const float *prim; // 5 (2D) or 16 (3D) arrays of npad floats
+    const int *wide2bin;
+};
+
+struct WideResult {
+    float best;   // squared distance
+    int slot;     // wide slot of the closest primitive
+};
+
+__device__ __forceinline__ unsigned order_key(float d, unsigned lane) {
+    // non-negative floats order like their bit patterns; the low 5 bits name
+    // the lane so keys are unique (ties broken towards the lower lane)
+    return (__float_as_uint(d) & ~31u) | lane;
+}
+
+template <int DIM>
+__device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int idx, float px,
+                                               float py, float pz) {
+    const int t = w.box_total;
+    const float *b = w.box + w.off[h] + idx;
+    const float lx = b[0], ly = b[t];
+    float dx, dy;
+    if (DIM == 2) {
+        const float hx = b[2 * t], hy = b[3 * t];
+        dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
+        dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
+        return dx * dx + dy * dy;
+    }
+    const float lz = b[2 * t], hx = b[3 * t], hy = b[4 * t], hz = b[5 * t];
+    dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
+    dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
+    const float dz = fmaxf(0.0f, fmaxf(lz - pz, pz - hz));
+    return dx * dx + dy * dy + dz * dz;
+}
+
+template <int DIM>
+__device__ __forceinline__ float wide_prim_dist(const WideView &w, int s, float px, float py,
+                                                float pz) {
+    const int np = w.npad;
+    const float *r = w.prim + s;
+    if (DIM == 2) {
+        const float x0 = r[0], y0 = r[np], vx = r[2 * np], vy = r[3 * np], inv = r[4 * np];
+        const float wx = px - x0, wy = py - y0;
+        const float t = fminf(fmaxf((wx * vx + wy * vy) * inv, 0.0f), 1.0f);
+        const float dx = wx - t * vx, dy = wy - t * vy;
+        return dx * dx + dy * dy;
+    }
+    float4 rec[4];
+    float *f = reinterpret_cast<float *>(rec);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) f[k] = r[k * np];
+    return eberly32(px, py, pz, rec);
+}
+
+// Closest primitive to (px, py, pz); all 32 lanes of the warp must call this
+// with the same point and receive the same result.
+template <int DIM>
+__device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, float py,
+                                                   float pz, float keep, float exact2) {
+    constexpr unsigned kAll = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    float best = INFINITY, limit = INFINITY;
+    int slot = -1;
+    auto leaf = [&](int cluster) {
+        const int s = cluster * 32 + static_cast<int>(lane);
+        const float d2 = wide_prim_dist<DIM>(w, s, px, py, pz);
+        const unsigned u = __reduce_min_sync(kAll, __float_as_uint(d2));
+        const float m = __uint_as_float(u);
+        if (m < best) {
+            best = m;
+            slot = cluster * 32 + (__ffs(__ballot_sync(kAll, __float_as_uint(d2) == u)) - 1);
+            limit = best > exact2 ? best * keep : best;
+        }
+    };
+    if (w.H == 1) {
+        leaf(0);
+        return WideResult{best, slot};
+    }
+    int h = w.H;    // height of the current node
+    int node = 0;   // its index at that height
+    float d = wide_box_dist<DIM>(w, h - 1, static_cast<int>(lane), px, py, pz);
+    unsigned m = __ballot_sync(kAll, d < limit);
+    for (;;) {
+        if (m == 0u) {
+            if (h == w.H) break;
+            // back to the parent: its children with a key above ours are pending
+            const unsigned left = static_cast<unsigned>(node) & 31u;
+            node >>= 5;
+            ++h;
+            d = wide_box_dist<DIM>(w, h - 1, node * 32 + static_cast<int>(lane), px, py, pz);
+            const unsigned key = order_key(d, lane);
+            const unsigned key_left = __shfl_sync(kAll, key, left);
+            m = __ballot_sync(kAll, key > key_left && d < limit);
+            continue;
+        }
+        const unsigned key = ((m >> lane) & 1u) ? order_key(d, lane) : 0xffffffffu;
+        const unsigned k = __reduce_min_sync(kAll, key) & 31u;
+        m &= ~(1u << k);
+        const int child = node * 32 + static_cast<int>(k);
+        if (h == 2) {
+            leaf(child);
+            m &= __ballot_sync(kAll, d < limit);
+        } else {
+            node = child;
+            --h;
+            d = wide_box_dist<DIM>(w, h - 1, node * 32 + static_cast<int>(lane), px, py, pz);
+            m = __ballot_sync(kAll, d < limit);
+        }
+    }
+    return WideResult{best, slot};
+}
+
+}  // namespace wosb

@@ -32,7 +32,8 @@ struct FastPlan {
     long long n_tasks;    // points * chunks
     int blocks;           // persistent grid size
     int threads;          // block size
-    bool stage_scene;     // copy the FP32 scene into shared memory
+    bool stage_scene;     // copy the wide FP32 boxes into shared memory
+    bool stage_prims;     // ... and the wide FP32 primitives
     int smem_bytes;
 };
 
@@ -48,22 +49,24 @@ struct TaskPartial {
 
 // FAST_FP32 (precision 32) / FAST_FP64 (precision 64) walks over all tasks,
 // then the per-point merge into the output fields.
-cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t seed, EqDesc eq,
+cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointSet &ps,
+                             uint64_t seed, EqDesc eq,
                              int n_walks, double epsilon, int max_steps, double shell_delta,
                              int precision, const FastPlan &plan, const uint8_t *location,
                              const StartRecord *start, TaskPartial *partials,
                              unsigned long long *queue, Fields out, DeviceCounters *counters,
                              cudaStream_t stream, cudaEvent_t after_walk = nullptr);
 
-FastPlan plan_fast(const SceneView &s, long long n_points, int n_walks, int precision,
-                   int device_sms, size_t smem_optin);
+FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, int n_walks,
+                   int precision, int device_sms, size_t smem_optin);
 
 // Kernel-level checks.
 cudaError_t launch_prng(const uint64_t *seeds, long long n, int count, uint64_t *out,
                         cudaStream_t stream);
 cudaError_t launch_closest64(const SceneView &s, const double *pts, long long n, double *dist,
                              double *nearest, int *boundary_id, cudaStream_t stream);
-cudaError_t launch_closest32(const SceneView &s, const double *pts, long long n, double *dist,
-                             double *nearest, int *boundary_id, cudaStream_t stream);
+cudaError_t launch_closest32(const SceneView &s, const WideView &w, const double *pts,
+                             long long n, double *dist, double *nearest, int *boundary_id,
+                             cudaStream_t stream);
 
 }  // namespace wosb

@@ -17,6 +17,7 @@
 // boundary id for the boundary value, evaluated in FP64.  Per-walk values are
 // accumulated in FP64 (Welford per lane, Chan's merge across lanes and
 // chunks).  FAST_FP64 runs the same scheduling with FP64 everywhere.
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 
@@ -42,6 +43,7 @@ __device__ __forceinline__ double FastRng<double>::unit() { return s.uniform_d()
 
 struct FastArgs {
     SceneView s;
+    WideView w;
     PointSet ps;
     uint64_t seed;
     int n_walks;
@@ -56,9 +58,8 @@ struct FastArgs {
     int chunks;
     long long n_tasks;
     int stage;
-    int pair_f4;   // float4 count of the pair array (staged)
-    int prim_f4;   // float4 count of the primitive array (staged)
-    int aux_f4;    // float4 count of the 2D reciprocal array (staged)
+    int stage_box;   // floats of the wide box arrays staged in shared memory
+    int stage_prim;  // floats of the wide primitive arrays staged (0: read from global)
     const uint8_t *location;
     const StartRecord *start;
     TaskPartial *partials;
@@ -95,6 +96,7 @@ __device__ __forceinline__ int bid_of(const SceneView &s, int slot) {
 template <int DIM>
 __device__ __forceinline__ double reproject64(const SceneView &s, int slot, double px, double py,
                                               double pz, V3<double> &np, int &bid) {
+    // `slot` is a binary-tree slot (the FP64 records' order)
     if (DIM == 2) {
         const double2 a = s.seg64[2 * slot], c = s.seg64[2 * slot + 1];
         double nx, ny;
@@ -113,24 +115,24 @@ __device__ __forceinline__ double reproject64(const SceneView &s, int slot, doub
     return sqrt(d2);
 }
 
-template <int DIM, class Eq, typename T>
-__global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
+template <int DIM, class Eq, typename T, int MIN_BLOCKS>
+__global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, Eq eq) {
     constexpr bool kF32 = std::is_same<T, float>::value;
     extern __shared__ float4 smem[];
-    const float4 *pairs = a.s.pair32;
-    const float4 *prims = DIM == 2 ? a.s.seg32 : a.s.tri32;
-    const float *inv = a.s.seg32inv;
+    __shared__ int s_off[8];
+    if (threadIdx.x < 8) s_off[threadIdx.x] = a.w.off[threadIdx.x];
+    WideView wv = a.w;
+    wv.off = s_off;
+    if (!kF32 || !a.stage) __syncthreads();
     if (kF32 && a.stage) {
-        for (int i = threadIdx.x; i < a.pair_f4; i += blockDim.x) smem[i] = pairs[i];
-        for (int i = threadIdx.x; i < a.prim_f4; i += blockDim.x) smem[a.pair_f4 + i] = prims[i];
-        float *aux = reinterpret_cast<float *>(smem + a.pair_f4 + a.prim_f4);
-        if (DIM == 2) {
-            for (int i = threadIdx.x; i < a.s.n_prims; i += blockDim.x) aux[i] = inv[i];
+        float *sm = reinterpret_cast<float *>(smem);
+        for (int i = threadIdx.x; i < a.stage_box; i += blockDim.x) sm[i] = a.w.box[i];
+        for (int i = threadIdx.x; i < a.stage_prim; i += blockDim.x) {
+            sm[a.stage_box + i] = a.w.prim[i];
         }
         __syncthreads();
-        pairs = smem;
-        prims = smem + a.pair_f4;
-        inv = aux;
+        wv.box = sm;
+        if (a.stage_prim) wv.prim = sm + a.stage_box;
     }
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -177,6 +179,7 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
 
         while (__any_sync(kFull, active)) {
             bool done = false;
+            bool need_query = false;
             double value = 0.0;
             if (active) {
                 bool stop = false;
@@ -195,7 +198,8 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                     bid = bid64;
                 } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
                     // epsilon shell: FP64 re-projection onto the nearest primitive
-                    const double d64 = reproject64<DIM>(a.s, slot, static_cast<double>(p.x),
+                    const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
+                                                        static_cast<double>(p.x),
                                                         static_cast<double>(p.y),
                                                         static_cast<double>(p.z), np, bid);
                     if (d64 <= eps) {
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                     ++hits;
                     stop = true;
                     if (kF32) {
-                        reproject64<DIM>(a.s, slot, static_cast<double>(p.x),
+                        reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
                                          static_cast<double>(p.y), static_cast<double>(p.z), np,
                                          bid);
                     } else {
@@ -226,12 +230,7 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                     p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
                     ++steps;
                     if constexpr (kF32) {
-                        const Nearest32 q = nearest32<DIM>(pairs, prims, inv, a.s.n_prims,
-                                                           a.s.depth, p.x, p.y, p.z, a.keep,
-                                                           a.exact2);
-                        const float r = sqrtf(q.best);
-                        R = q.best > a.shell2 ? r * a.shrink : r;
-                        slot = q.slot;
+                        need_query = true;
                     } else {
                         const Nearest<double> q = nearest64<DIM>(
                             a.s, static_cast<double>(p.x), static_cast<double>(p.y),
@@ -240,6 +239,29 @@ __global__ void __launch_bounds__(256) walk_fast_kernel(FastArgs a, Eq eq) {
                         np64 = V3<double>{q.x, q.y, q.z};
                         bid64 = bid_of<DIM>(a.s, q.slot);
                     }
+                }
+            }
+            if constexpr (kF32) {
+                // the warp resolves every pending closest-point query together
+                unsigned pending = __ballot_sync(kFull, need_query);
+                float qbest = 0.0f;
+                int qslot = -1;
+                while (pending) {
+                    const int j = __ffs(pending) - 1;
+                    pending &= pending - 1u;
+                    const float qx = __shfl_sync(kFull, static_cast<float>(p.x), j);
+                    const float qy = __shfl_sync(kFull, static_cast<float>(p.y), j);
+                    const float qz = DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), j) : 0.0f;
+                    const WideResult r = wide_nearest<DIM>(wv, qx, qy, qz, a.keep, a.exact2);
+                    if (lane == j) {
+                        qbest = r.best;
+                        qslot = r.slot;
+                    }
+                }
+                if (need_query) {
+                    const float r = sqrtf(qbest);
+                    R = static_cast<T>(qbest > a.shell2 ? r * a.shrink : r);
+                    slot = qslot;
                 }
             }
             if (done) {
@@ -325,29 +347,44 @@ __global__ void merge_kernel(long long n_points, int chunks, int n_walks,
     }
 }
 
-template <int DIM, typename T>
-__global__ void closest32_kernel(SceneView s, const double *pts, long long n, double *dist,
-                                 double *nearest, int *bid) {
-    const float4 *pairs = s.pair32;
-    const float4 *prims = DIM == 2 ? s.seg32 : s.tri32;
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
-         t += stride) {
-        const float px = static_cast<float>(pts[DIM * t]);
-        const float py = static_cast<float>(pts[DIM * t + 1]);
-        const float pz = DIM == 3 ? static_cast<float>(pts[DIM * t + 2]) : 0.0f;
-        // exact FP32 query (keep = 1), nearest point by FP64 re-projection
-        const Nearest32 q = nearest32<DIM>(pairs, prims, s.seg32inv, s.n_prims, s.depth, px, py,
-                                           pz, 1.0f, 0.0f);
-        dist[t] = sqrtf(q.best);
-        V3<double> np;
-        int b = -1;
-        reproject64<DIM>(s, q.slot, px, py, pz, np, b);
-        nearest[DIM * t] = np.x;
-        nearest[DIM * t + 1] = np.y;
-        if (DIM == 3) nearest[DIM * t + 2] = np.z;
-        if (bid) bid[t] = b;
+template <int DIM>
+__global__ void closest32_kernel(SceneView s, WideView w, const double *pts, long long n,
+                                 double *dist, double *nearest, int *bid) {
+    // each warp takes 32 queries and resolves them one after another
+    const long long base = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ll;
+    const int lane = threadIdx.x & 31;
+    const long long t = base + lane;
+    const bool valid = t < n;
+    float px = 0.0f, py = 0.0f, pz = 0.0f;
+    if (valid) {
+        px = static_cast<float>(pts[DIM * t]);
+        py = static_cast<float>(pts[DIM * t + 1]);
+        pz = DIM == 3 ? static_cast<float>(pts[DIM * t + 2]) : 0.0f;
     }
+    float mybest = 0.0f;
+    int myslot = -1;
+    unsigned pending = __ballot_sync(kFull, valid);
+    while (pending) {
+        const int j = __ffs(pending) - 1;
+        pending &= pending - 1u;
+        const float qx = __shfl_sync(kFull, px, j), qy = __shfl_sync(kFull, py, j);
+        const float qz = __shfl_sync(kFull, pz, j);
+        // exact query (keep = 1)
+        const WideResult r = wide_nearest<DIM>(w, qx, qy, qz, 1.0f, 0.0f);
+        if (lane == j) {
+            mybest = r.best;
+            myslot = r.slot;
+        }
+    }
+    if (!valid) return;
+    dist[t] = sqrtf(mybest);
+    V3<double> np;
+    int b = -1;
+    reproject64<DIM>(s, w.wide2bin[myslot], px, py, pz, np, b);
+    nearest[DIM * t] = np.x;
+    nearest[DIM * t + 1] = np.y;
+    if (DIM == 3) nearest[DIM * t + 2] = np.z;
+    if (bid) bid[t] = b;
 }
 
 template <int DIM, class Eq>
@@ -373,7 +410,7 @@ cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
     };
     int blocks = 0;
     if (precision == 32) {
-        auto k = walk_fast_kernel<DIM, Eq, float>;
+        auto k = walk_fast_kernel<DIM, Eq, float, 3>;
         if (plan.smem_bytes > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  plan.smem_bytes);
@@ -383,7 +420,7 @@ cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
         if (e != cudaSuccess) return e;
         k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq);
     } else {
-        auto k = walk_fast_kernel<DIM, Eq, double>;
+        auto k = walk_fast_kernel<DIM, Eq, double, 1>;
         cudaError_t e = grid_for(k, 0, blocks);
         if (e != cudaSuccess) return e;
         k<<<blocks, plan.threads, 0, stream>>>(a, eq);
@@ -410,26 +447,30 @@ cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const Fa
 
 }  // namespace
 
-FastPlan plan_fast(const SceneView &s, long long n_points, int n_walks, int precision,
-                   int device_sms, size_t smem_optin) {
+FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, int n_walks,
+                   int precision, int device_sms, size_t smem_optin) {
     FastPlan p{};
     p.threads = 256;
     p.chunk = n_walks < 1024 ? n_walks : 1024;
     if (p.chunk < 1) p.chunk = 1;
     p.chunks = (n_walks + p.chunk - 1) / p.chunk;
     p.n_tasks = n_points * p.chunks;
-    const int pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
-    const int prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
-    const int aux_f4 = s.dim == 2 ? (s.n_prims + 3) / 4 : 0;
-    const size_t bytes = static_cast<size_t>(pair_f4 + prim_f4 + aux_f4) * sizeof(float4);
-    p.stage_scene = precision == 32 && bytes <= 96 * 1024 && bytes <= smem_optin;
-    p.smem_bytes = p.stage_scene ? static_cast<int>(bytes) : 0;
+    // stage the wide boxes, and the primitives too when they fit, in shared memory
+    const size_t box_floats = static_cast<size_t>(2 * w.dim) * w.box_total;
+    const size_t prim_floats = static_cast<size_t>(w.dim == 2 ? 5 : 16) * w.npad;
+    const size_t cap = std::min<size_t>(96 * 1024, smem_optin);
+    p.stage_scene = precision == 32 && box_floats * 4 <= cap;
+    p.stage_prims = p.stage_scene && (box_floats + prim_floats) * 4 <= cap;
+    p.smem_bytes = p.stage_scene
+                       ? static_cast<int>((box_floats + (p.stage_prims ? prim_floats : 0)) * 4)
+                       : 0;
     (void)device_sms;
     p.blocks = 0;  // sized from the occupancy of the chosen kernel at launch
     return p;
 }
 
-cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t seed, EqDesc eq,
+cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointSet &ps,
+                             uint64_t seed, EqDesc eq,
                              int n_walks, double epsilon, int max_steps, double shell_delta,
                              int precision, const FastPlan &plan, const uint8_t *location,
                              const StartRecord *start, TaskPartial *partials,
@@ -447,10 +488,10 @@ cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t se
     a.chunk = plan.chunk;
     a.chunks = plan.chunks;
     a.n_tasks = plan.n_tasks;
+    a.w = w;
     a.stage = plan.stage_scene ? 1 : 0;
-    a.pair_f4 = (1 << s.depth) * (s.dim == 2 ? 2 : 3);
-    a.prim_f4 = s.n_prims * (s.dim == 2 ? 1 : 4);
-    a.aux_f4 = s.dim == 2 ? (s.n_prims + 3) / 4 : 0;
+    a.stage_box = plan.stage_scene ? 2 * w.dim * w.box_total : 0;
+    a.stage_prim = plan.stage_prims ? (w.dim == 2 ? 5 : 16) * w.npad : 0;
     // FP32 queries are conservative to a relative tau = 2^-10 outside the
     // epsilon shell and exact inside it (see Nearest32)
     const double tau = 1.0 / 1024.0;
@@ -480,16 +521,17 @@ cudaError_t launch_walk_fast(const SceneView &s, const PointSet &ps, uint64_t se
     return cudaGetLastError();
 }
 
-cudaError_t launch_closest32(const SceneView &s, const double *pts, long long n, double *dist,
-                             double *nearest, int *bid, cudaStream_t stream) {
+cudaError_t launch_closest32(const SceneView &s, const WideView &w, const double *pts,
+                             long long n, double *dist, double *nearest, int *bid,
+                             cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     long long b = (n + 127) / 128;
     if (s.dim == 2) {
-        closest32_kernel<2, float><<<static_cast<int>(b), 128, 0, stream>>>(s, pts, n, dist,
-                                                                           nearest, bid);
+        closest32_kernel<2><<<static_cast<int>(b), 128, 0, stream>>>(s, w, pts, n, dist, nearest,
+                                                                     bid);
     } else {
-        closest32_kernel<3, float><<<static_cast<int>(b), 128, 0, stream>>>(s, pts, n, dist,
-                                                                           nearest, bid);
+        closest32_kernel<3><<<static_cast<int>(b), 128, 0, stream>>>(s, w, pts, n, dist, nearest,
+                                                                     bid);
     }
     return cudaGetLastError();
 }

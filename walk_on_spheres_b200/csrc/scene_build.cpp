@@ -87,7 +87,152 @@ struct Builder {
     }
 };
 
+// 32-wide tree: the node at height h covering [s, e) is split into children
+// of 32^(h-1) slots by recursive median bisection along the longest axis, with
+// split points on multiples of the child size.
+struct WideBuilder {
+    int dim;
+    std::vector<Item> &items;
+
+    void bbox(int s, int e, double *lo, double *hi) const {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = items[s].lo[k];
+            hi[k] = items[s].hi[k];
+        }
+        for (int i = s + 1; i < e; ++i) {
+            for (int k = 0; k < dim; ++k) {
+                lo[k] = std::min(lo[k], items[i].lo[k]);
+                hi[k] = std::max(hi[k], items[i].hi[k]);
+            }
+        }
+    }
+
+    void split(int s, int e, long long chunk, int child_height) {
+        const long long nch = (e - s + chunk - 1) / chunk;
+        if (nch <= 1) {
+            node(s, e, child_height);
+            return;
+        }
+        const int mid = static_cast<int>(s + ((nch + 1) / 2) * chunk);
+        double lo[3], hi[3];
+        bbox(s, e, lo, hi);
+        const double ex = hi[0] - lo[0], ey = hi[1] - lo[1];
+        const double ez = dim == 3 ? hi[2] - lo[2] : -1.0;
+        const int axis = (ex >= ey) ? (ex >= ez ? 0 : 2) : (ey >= ez ? 1 : 2);
+        std::nth_element(items.begin() + s, items.begin() + mid, items.begin() + e,
+                         [axis](const Item &x, const Item &y) {
+                             if (x.c[axis] < y.c[axis]) return true;
+                             if (x.c[axis] > y.c[axis]) return false;
+                             return x.prim < y.prim;
+                         });
+        split(s, mid, chunk, child_height);
+        split(mid, e, chunk, child_height);
+    }
+
+    void node(int s, int e, int height) {
+        if (height <= 1) {
+            std::sort(items.begin() + s, items.begin() + e,
+                      [](const Item &x, const Item &y) { return x.prim < y.prim; });
+            return;
+        }
+        long long chunk = 1;
+        for (int h = 1; h < height; ++h) chunk *= 32;
+        split(s, e, chunk, height - 1);
+    }
+};
+
 }  // namespace
+
+static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
+    const int n = sc.n_prims;
+    int H = 1;
+    long long span = 32;
+    while (span < n) {
+        span *= 32;
+        ++H;
+    }
+    sc.wH = H;
+    WideBuilder W{dim, items};
+    W.node(0, n, H);
+    sc.w_npad = (n + 31) / 32 * 32;
+
+    // binary slot of every primitive (for the FP64 records)
+    std::vector<int> bin_of(n);
+    for (int s = 0; s < n; ++s) bin_of[sc.order[s]] = s;
+    sc.wide2bin.assign(sc.w_npad, -1);
+    for (int s = 0; s < n; ++s) sc.wide2bin[s] = bin_of[items[s].prim];
+
+    // node boxes per height (FP64, then rounded outward and widened)
+    const int nc = 2 * dim;
+    std::vector<std::vector<double>> lv(H + 1);
+    std::vector<long long> cnt(H + 1);
+    cnt[0] = n;
+    lv[0].resize(static_cast<size_t>(n) * nc);
+    for (int s = 0; s < n; ++s) {
+        for (int k = 0; k < dim; ++k) {
+            lv[0][static_cast<size_t>(s) * nc + k] = items[s].lo[k];
+            lv[0][static_cast<size_t>(s) * nc + dim + k] = items[s].hi[k];
+        }
+    }
+    for (int h = 1; h <= H; ++h) {
+        cnt[h] = (cnt[h - 1] + 31) / 32;
+        lv[h].assign(static_cast<size_t>(cnt[h]) * nc, 0.0);
+        for (long long i = 0; i < cnt[h]; ++i) {
+            const long long c0 = 32 * i, c1 = std::min(cnt[h - 1], 32 * i + 32);
+            for (int k = 0; k < nc; ++k) {
+                double v = lv[h - 1][static_cast<size_t>(c0) * nc + k];
+                for (long long c = c0 + 1; c < c1; ++c) {
+                    const double x = lv[h - 1][static_cast<size_t>(c) * nc + k];
+                    v = k < dim ? std::min(v, x) : std::max(v, x);
+                }
+                lv[h][static_cast<size_t>(i) * nc + k] = v;
+            }
+        }
+    }
+    // heights 1..H-1 are children of some node: 32 * cnt[h+1] entries each
+    int total = 0;
+    for (int h = 1; h < H; ++h) {
+        sc.w_off[h] = total;
+        total += static_cast<int>(32 * cnt[h + 1]);
+    }
+    sc.w_box_total = std::max(total, 32);
+    const double widen = std::ldexp(sc.scale, -20);
+    sc.wbox.assign(static_cast<size_t>(nc) * sc.w_box_total, 0.0f);
+    for (int c = 0; c < nc; ++c) {
+        float *arr = sc.wbox.data() + static_cast<size_t>(c) * sc.w_box_total;
+        // padding boxes are empty (lo = +inf, hi = -inf): infinitely far
+        for (int i = 0; i < sc.w_box_total; ++i) arr[i] = c < dim ? INFINITY : -INFINITY;
+    }
+    for (int h = 1; h < H; ++h) {
+        for (long long i = 0; i < cnt[h]; ++i) {
+            for (int k = 0; k < nc; ++k) {
+                const double v = lv[h][static_cast<size_t>(i) * nc + k];
+                sc.wbox[static_cast<size_t>(k) * sc.w_box_total + sc.w_off[h] + i] =
+                    k < dim ? round_down(v - widen) : round_up(v + widen);
+            }
+        }
+    }
+    // primitive SoA in wide-slot order; padding primitives are far away
+    const int na = dim == 2 ? 5 : 16;
+    const size_t np = static_cast<size_t>(sc.w_npad);
+    sc.wprim.assign(np * na, 0.0f);
+    for (int s = 0; s < sc.w_npad; ++s) {
+        float rec[16];
+        if (s >= n) {
+            for (float &x : rec) x = 0.0f;
+            rec[0] = rec[1] = 1e30f;
+            if (dim == 3) rec[2] = 1e30f;
+        } else if (dim == 2) {
+            const int b = sc.wide2bin[s];
+            for (int k = 0; k < 4; ++k) rec[k] = sc.seg32[4 * static_cast<size_t>(b) + k];
+            rec[4] = sc.seg32inv[b];
+        } else {
+            const int b = sc.wide2bin[s];
+            for (int k = 0; k < 16; ++k) rec[k] = sc.tri32[16 * static_cast<size_t>(b) + k];
+        }
+        for (int k = 0; k < na; ++k) sc.wprim[static_cast<size_t>(k) * np + s] = rec[k];
+    }
+}
 
 std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                         const int *boundary_ids, int leaf_size, HostScene &sc) {
@@ -272,6 +417,7 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
             o[15] = static_cast<float>(1.0 / fc);
         }
     }
+    build_wide(sc, B.items, dim);
     return std::string();
 }
 

@@ -23,6 +23,15 @@ struct HostScene {
     std::vector<float> seg32inv; // 2D: 1/|v|^2 per slot
     std::vector<float> tri32;    // 3D: {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}
     std::vector<int> order;      // leaf slot -> primitive id
+    // 32-wide FP32 tree (device/wide.cuh): heights 1..wH-1 of child boxes,
+    // primitives in wide-slot order, all SoA
+    int wH = 1;                  // root height (32^wH >= n_prims)
+    int w_npad = 0;              // primitive slots padded to a multiple of 32
+    int w_box_total = 0;         // boxes per coordinate array
+    int w_off[8] = {0};          // offset of height h's boxes in each coordinate array
+    std::vector<float> wbox;     // dim*2 arrays of w_box_total: lo.x lo.y [lo.z] hi.x hi.y [hi.z]
+    std::vector<float> wprim;    // 2D: x0 y0 vx vy inv; 3D: v0 e1 e2 a b c det 1/det 1/a 1/c (16)
+    std::vector<int> wide2bin;   // wide slot -> binary-tree slot (FP64 records), -1 for padding
     // the mesh itself (for the adjoint's per-vertex data and the checks)
     std::vector<double> verts;
     std::vector<int> prims;
