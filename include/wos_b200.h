@@ -228,6 +228,15 @@ int wos_read_obj(const char *path, int *dim, int *n_verts, int *n_prims, double 
 int wos_build_bvh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                   int leaf_size, int *depth, double *node_boxes, int *order);
 
+/* Host build of the FP32 32-wide tree used by the FAST_FP32 walks (no
+ * counterpart in the reference): root height H (32^H >= n_prims), entries per
+ * node array, the node arrays (3*dim+2 float arrays of that many entries: box
+ * lo[dim], hi[dim], slab normal[dim], slab offset, slab half-thickness; height
+ * h starts at offsets[h]) and the wide-slot primitive order.  Pass null arrays
+ * to get the sizes. */
+int wos_build_wide_bvh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                       int *height, int *entries, int *offsets, float *nodes, int *order);
+
 /* Write a result file with the reference's HDF5 layout (wos_write_hdf5,
  * include/wos/hdf5_io.hpp:15-338): /mean /variance /standard_error
  * /mean_steps (f64 [Nx,Ny,Nz]), /location (u8), /x /y /z and the /metadata

@@ -216,3 +216,47 @@ def test_hdf5_result_layout(tmp_path, dim):
     assert ("ambiguous_ray_retries" in m) == (dim == 3)
     if dim == 3:
         assert m["max_ray_attempts"] == 12 and m["indeterminate_points"] == 2
+
+
+def build_wide(m):
+    L = _lib.lib()
+    verts = np.ascontiguousarray(m.verts)
+    prims = np.ascontiguousarray(m.prims, dtype=np.int32)
+    H, E = C.c_int(), C.c_int()
+    offs = np.zeros(8, dtype=np.int32)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert L.wos_build_wide_bvh(m.dim, vp(verts), verts.shape[0], vp(prims), prims.shape[0],
+                                C.byref(H), C.byref(E), vp(offs), None, None) == 0
+    nodes = np.zeros(((3 * m.dim + 2), E.value), dtype=np.float32)
+    order = np.zeros(m.n_prims, dtype=np.int32)
+    L.wos_build_wide_bvh(m.dim, vp(verts), verts.shape[0], vp(prims), prims.shape[0],
+                         C.byref(H), C.byref(E), vp(offs), vp(nodes), vp(order))
+    return H.value, offs, nodes, order
+
+
+@pytest.mark.parametrize("mname", ["annulus", "circle1024", "sphere", "star", "pert"])
+def test_wide_bvh_bounds_contain_primitives(mname):
+    rng = np.random.default_rng(3)
+    m = {"annulus": meshes.annulus(), "circle1024": meshes.circle(segments=1024),
+         "sphere": meshes.uv_sphere(lon=48, lat=24),
+         "star": meshes.star_polygon(rng, 3000),
+         "pert": meshes.perturbed_sphere(rng, 40, 20)}[mname]
+    H, offs, nodes, order = build_wide(m)
+    n, d = m.n_prims, m.dim
+    assert sorted(order.tolist()) == list(range(n))
+    assert 32 ** H >= n and (H == 1 or 32 ** (H - 1) < n)
+    V = m.verts[m.prims[order]].astype(np.float64)          # (n, dim, dim) in wide-slot order
+    for h in range(1, H):
+        span = 32 ** h
+        count = -(-n // span)
+        for i in range(count):
+            pts = V[i * span:min(n, (i + 1) * span)].reshape(-1, d)
+            col = nodes[:, offs[h] + i].astype(np.float64)
+            lo, hi = col[:d], col[d:2 * d]
+            nrm, c, th = col[2 * d:3 * d], col[3 * d], col[3 * d + 1]
+            assert (pts >= lo).all() and (pts <= hi).all()
+            # the slab test as the device evaluates it, in float32
+            t = np.abs((pts.astype(np.float32) * nrm.astype(np.float32)).sum(axis=1,
+                       dtype=np.float32) - np.float32(c))
+            assert (t <= np.float32(th)).all(), (h, i, t.max(), th)
+            assert abs(np.linalg.norm(nrm) - 1.0) < 1e-5

@@ -82,6 +82,7 @@ SIGNATURES = {
     "wos_prng_u64": (C.c_int, [VP, VP, C.c_longlong, C.c_int, VP]),
     "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_build_wide_bvh": (C.c_int, [C.c_int, VP, C.c_int, VP, C.c_int] + [VP] * 5),
     "wos_equation_registry": (C.POINTER(EquationEntry), [C.POINTER(C.c_int)]),
     "wos_peek_mesh_dim": (C.c_int, [C.c_char_p]),
 }

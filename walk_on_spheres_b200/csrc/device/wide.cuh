@@ -33,7 +33,7 @@ struct WideView {
     int npad;          // primitive slots (multiple of 32)
     int box_total;     // entries per box coordinate array
     const int *off;    // [8]: offset of height h in each box coordinate array
-    const float *box;  // 2*dim arrays of box_total floats
+    const float *box;  // 3*dim+2 arrays of box_total floats: lo, hi, slab normal, c, h
     const float *prim; // 5 (2D) or 16 (3D) arrays of npad floats
     const int *wide2bin;
 };
@@ -49,6 +49,9 @@ __device__ __forceinline__ unsigned order_key(float d, unsigned lane) {
     return (__float_as_uint(d) & ~31u) | lane;
 }
 
+// Squared lower bound of the distance from p to the primitives of a node: the
+// larger of the box distance and the distance outside the node's slab
+// {x : |n.x - c| <= h}.
 template <int DIM>
 __device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int idx, float px,
                                                float py, float pz) {
@@ -58,15 +61,19 @@ __device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int idx
     float dx, dy;
     if (DIM == 2) {
         const float hx = b[2 * t], hy = b[3 * t];
+        const float nx = b[4 * t], ny = b[5 * t], c = b[6 * t], th = b[7 * t];
         dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
         dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
-        return dx * dx + dy * dy;
+        const float ds = fmaxf(0.0f, fabsf(nx * px + ny * py - c) - th);
+        return fmaxf(dx * dx + dy * dy, ds * ds);
     }
     const float lz = b[2 * t], hx = b[3 * t], hy = b[4 * t], hz = b[5 * t];
+    const float nx = b[6 * t], ny = b[7 * t], nz = b[8 * t], c = b[9 * t], th = b[10 * t];
     dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
     dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
     const float dz = fmaxf(0.0f, fmaxf(lz - pz, pz - hz));
-    return dx * dx + dy * dy + dz * dz;
+    const float ds = fmaxf(0.0f, fabsf(nx * px + ny * py + nz * pz - c) - th);
+    return fmaxf(dx * dx + dy * dy + dz * dz, ds * ds);
 }
 
 template <int DIM>

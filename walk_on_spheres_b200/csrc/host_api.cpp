@@ -62,6 +62,23 @@ extern "C" int wos_build_bvh(int dim, const double *verts, int n_verts, const in
     return WOS_OK;
 }
 
+extern "C" int wos_build_wide_bvh(int dim, const double *verts, int n_verts, const int *prims,
+                                  int n_prims, int *height, int *entries, int *offsets,
+                                  float *nodes, int *order) {
+    wosb::HostScene sc;
+    const std::string err =
+        wosb::build_scene(dim, verts, n_verts, prims, n_prims, nullptr, 0, sc);
+    if (!err.empty()) return WOS_ERR_MESH;
+    if (height) *height = sc.wH;
+    if (entries) *entries = sc.w_box_total;
+    if (offsets) std::memcpy(offsets, sc.w_off, sizeof(sc.w_off));
+    if (nodes) std::memcpy(nodes, sc.wbox.data(), sc.wbox.size() * sizeof(float));
+    if (order) {
+        for (int s = 0; s < n_prims; ++s) order[s] = sc.order[sc.wide2bin[s]];
+    }
+    return WOS_OK;
+}
+
 extern "C" int wos_write_hdf5(const char *path, const wos_grid *grid, const double *mean,
                               const double *variance, const double *standard_error,
                               const double *mean_steps, const uint8_t *location, int N_walks,

@@ -143,6 +143,69 @@ struct WideBuilder {
 
 }  // namespace
 
+// Principal plane of a point set: unit normal along the smallest-variance
+// direction (Jacobi eigen-decomposition of the covariance), offset n.mean and
+// half-thickness max |n.v - offset|.
+static void slab_of(const std::vector<double> &pts, int dim, double *n, double &c, double &h) {
+    const size_t m = pts.size() / dim;
+    double mean[3] = {0, 0, 0};
+    for (size_t i = 0; i < m; ++i)
+        for (int k = 0; k < dim; ++k) mean[k] += pts[i * dim + k];
+    for (int k = 0; k < dim; ++k) mean[k] /= static_cast<double>(m);
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (size_t i = 0; i < m; ++i)
+        for (int a = 0; a < dim; ++a)
+            for (int b = 0; b < dim; ++b)
+                A[a][b] += (pts[i * dim + a] - mean[a]) * (pts[i * dim + b] - mean[b]);
+    double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int sweep = 0; sweep < 32; ++sweep) {
+        double off = 0.0;
+        for (int a = 0; a < dim; ++a)
+            for (int b = a + 1; b < dim; ++b) off += A[a][b] * A[a][b];
+        if (off < 1e-30) break;
+        for (int a = 0; a < dim; ++a) {
+            for (int b = a + 1; b < dim; ++b) {
+                if (std::fabs(A[a][b]) < 1e-300) continue;
+                const double theta = 0.5 * std::atan2(2 * A[a][b], A[b][b] - A[a][a]);
+                const double cs = std::cos(theta), sn = std::sin(theta);
+                for (int k = 0; k < dim; ++k) {  // A <- A J
+                    const double x = A[k][a], y = A[k][b];
+                    A[k][a] = cs * x - sn * y;
+                    A[k][b] = sn * x + cs * y;
+                }
+                for (int k = 0; k < dim; ++k) {  // A <- J^T A
+                    const double x = A[a][k], y = A[b][k];
+                    A[a][k] = cs * x - sn * y;
+                    A[b][k] = sn * x + cs * y;
+                }
+                for (int k = 0; k < dim; ++k) {  // V <- V J
+                    const double x = V[k][a], y = V[k][b];
+                    V[k][a] = cs * x - sn * y;
+                    V[k][b] = sn * x + cs * y;
+                }
+            }
+        }
+    }
+    int best = 0;
+    for (int a = 1; a < dim; ++a)
+        if (A[a][a] < A[best][best]) best = a;
+    double len = 0.0;
+    for (int k = 0; k < dim; ++k) {
+        n[k] = V[k][best];
+        len += n[k] * n[k];
+    }
+    len = std::sqrt(len);
+    for (int k = 0; k < dim; ++k) n[k] /= len;
+    c = 0.0;
+    for (int k = 0; k < dim; ++k) c += n[k] * mean[k];
+    h = 0.0;
+    for (size_t i = 0; i < m; ++i) {
+        double t = -c;
+        for (int k = 0; k < dim; ++k) t += n[k] * pts[i * dim + k];
+        h = std::max(h, std::fabs(t));
+    }
+}
+
 static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
     const int n = sc.n_prims;
     int H = 1;
@@ -197,19 +260,62 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
     }
     sc.w_box_total = std::max(total, 32);
     const double widen = std::ldexp(sc.scale, -20);
-    sc.wbox.assign(static_cast<size_t>(nc) * sc.w_box_total, 0.0f);
-    for (int c = 0; c < nc; ++c) {
+    // per node: box lo[dim], hi[dim], then slab normal n[dim], offset c and
+    // half-thickness h (all SoA)
+    const int nbox = nc + dim + 2;
+    sc.wbox.assign(static_cast<size_t>(nbox) * sc.w_box_total, 0.0f);
+    for (int c = 0; c < nbox; ++c) {
         float *arr = sc.wbox.data() + static_cast<size_t>(c) * sc.w_box_total;
-        // padding boxes are empty (lo = +inf, hi = -inf): infinitely far
-        for (int i = 0; i < sc.w_box_total; ++i) arr[i] = c < dim ? INFINITY : -INFINITY;
+        // padding boxes are empty (lo = +inf, hi = -inf): infinitely far;
+        // their slab is unbounded (h = +inf)
+        float fill = 0.0f;
+        if (c < dim) fill = INFINITY;
+        else if (c < nc) fill = -INFINITY;
+        else if (c == nbox - 1) fill = INFINITY;
+        for (int i = 0; i < sc.w_box_total; ++i) arr[i] = fill;
     }
+    auto vertex = [&](int prim, int j, double *out) {
+        const int v = sc.prims[static_cast<size_t>(dim) * prim + j];
+        for (int k = 0; k < dim; ++k) out[k] = sc.verts[static_cast<size_t>(dim) * v + k];
+    };
+    std::vector<double> pts;
     for (int h = 1; h < H; ++h) {
+        long long span_h = 1;
+        for (int k = 0; k < h; ++k) span_h *= 32;
         for (long long i = 0; i < cnt[h]; ++i) {
             for (int k = 0; k < nc; ++k) {
                 const double v = lv[h][static_cast<size_t>(i) * nc + k];
                 sc.wbox[static_cast<size_t>(k) * sc.w_box_total + sc.w_off[h] + i] =
                     k < dim ? round_down(v - widen) : round_up(v + widen);
             }
+            // slab of every vertex of the node's primitives
+            pts.clear();
+            const long long s0 = i * span_h, s1 = std::min<long long>(n, (i + 1) * span_h);
+            for (long long sl = s0; sl < s1; ++sl) {
+                for (int j = 0; j < dim; ++j) {
+                    double v[3];
+                    vertex(items[sl].prim, j, v);
+                    pts.insert(pts.end(), v, v + dim);
+                }
+            }
+            double nrm[3] = {0, 0, 0}, c = 0.0, th = 0.0;
+            slab_of(pts, dim, nrm, c, th);
+            float nf[3];
+            for (int k = 0; k < dim; ++k) nf[k] = static_cast<float>(nrm[k]);
+            const float cf = static_cast<float>(c);
+            // thickness for the rounded normal and offset, padded for the FP32
+            // evaluation at query time
+            double t32 = 0.0;
+            for (size_t q = 0; q < pts.size() / dim; ++q) {
+                double t = -static_cast<double>(cf);
+                for (int k = 0; k < dim; ++k) t += static_cast<double>(nf[k]) * pts[q * dim + k];
+                t32 = std::max(t32, std::fabs(t));
+            }
+            const size_t at = static_cast<size_t>(sc.w_off[h] + i);
+            for (int k = 0; k < dim; ++k) sc.wbox[static_cast<size_t>(nc + k) * sc.w_box_total + at] = nf[k];
+            sc.wbox[static_cast<size_t>(nc + dim) * sc.w_box_total + at] = cf;
+            sc.wbox[static_cast<size_t>(nc + dim + 1) * sc.w_box_total + at] =
+                round_up(t32 + 4.0 * widen);
         }
     }
     // primitive SoA in wide-slot order; padding primitives are far away
