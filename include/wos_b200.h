@@ -229,11 +229,12 @@ int wos_build_bvh(int dim, const double *verts, int n_verts, const int *prims, i
                   int leaf_size, int *depth, double *node_boxes, int *order);
 
 /* Host build of the FP32 32-wide tree used by the FAST_FP32 walks (no
- * counterpart in the reference): root height H (32^H >= n_prims), entries per
- * node array, the node arrays (3*dim+2 float arrays of that many entries: box
- * lo[dim], hi[dim], slab normal[dim], slab offset, slab half-thickness; height
- * h starts at offsets[h]) and the wide-slot primitive order.  Pass null arrays
- * to get the sizes. */
+ * counterpart in the reference): root height H (32^H >= n_prims), the float
+ * count of the node blocks, the node blocks (the 32 children of a height-(h+1)
+ * node form a block of (3*dim+2) x 32 floats starting at offsets[h] + parent
+ * * (3*dim+2)*32: box lo[dim], hi[dim], slab normal[dim], slab offset, slab
+ * half-thickness, field f of child k at f*32 + k) and the wide-slot primitive
+ * order.  Pass null arrays to get the sizes. */
 int wos_build_wide_bvh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                        int *height, int *entries, int *offsets, float *nodes, int *order);
 

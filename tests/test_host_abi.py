@@ -227,7 +227,7 @@ def build_wide(m):
     vp = lambda a: a.ctypes.data_as(C.c_void_p)
     assert L.wos_build_wide_bvh(m.dim, vp(verts), verts.shape[0], vp(prims), prims.shape[0],
                                 C.byref(H), C.byref(E), vp(offs), None, None) == 0
-    nodes = np.zeros(((3 * m.dim + 2), E.value), dtype=np.float32)
+    nodes = np.zeros(E.value, dtype=np.float32)
     order = np.zeros(m.n_prims, dtype=np.int32)
     L.wos_build_wide_bvh(m.dim, vp(verts), verts.shape[0], vp(prims), prims.shape[0],
                          C.byref(H), C.byref(E), vp(offs), vp(nodes), vp(order))
@@ -251,7 +251,9 @@ def test_wide_bvh_bounds_contain_primitives(mname):
         count = -(-n // span)
         for i in range(count):
             pts = V[i * span:min(n, (i + 1) * span)].reshape(-1, d)
-            col = nodes[:, offs[h] + i].astype(np.float64)
+            nb = 3 * d + 2
+            blk = offs[h] + (i // 32) * nb * 32
+            col = nodes[blk + np.arange(nb) * 32 + i % 32].astype(np.float64)
             lo, hi = col[:d], col[d:2 * d]
             nrm, c, th = col[2 * d:3 * d], col[3 * d], col[3 * d + 1]
             assert (pts >= lo).all() and (pts <= hi).all()

@@ -4,11 +4,14 @@
 // recursive median bisection; the node at height h with index i covers slots
 // [i * 32^h, (i+1) * 32^h), so the children of node i are nodes 32i .. 32i+31
 // one height below and no pointers are stored.  The root has height H
-// (32^H >= n).  Child boxes of heights 1 .. H-1 and the primitives are stored
-// structure-of-arrays (one float array per coordinate / record field), so lane
-// k of a warp reads child k or slot k with conflict-free, coalesced accesses.
-// Padding boxes are empty (infinitely far) and padding primitives lie at
-// 1e30, so every lane always has something to test.
+// (32^H >= n).  Data are blocked by 32 (array of structures of arrays): the
+// 32 children of a node form one block of NB x 32 floats (field f of child k
+// at f*32 + k: box lo, hi, slab normal, slab offset, half-thickness) and the
+// 32 primitives of a leaf cluster one block of NF x 32 floats, so lane k of a
+// warp reads child k or slot k with one base address, immediate field
+// offsets and conflict-free 128-byte rows.  Padding children are empty
+// (infinitely far) and padding primitives lie at 1e30, so every lane always
+// has something to test.
 //
 // Traversal: one query at a time per warp, all 32 lanes working on it.  At a
 // node every lane computes the box distance of one child; the nearest pending
@@ -31,10 +34,10 @@ struct WideView {
     int H;             // root height
     int n;             // primitives
     int npad;          // primitive slots (multiple of 32)
-    int box_total;     // entries per box coordinate array
-    const int *off;    // [8]: offset of height h in each box coordinate array
-    const float *box;  // 3*dim+2 arrays of box_total floats: lo, hi, slab normal, c, h
-    const float *prim; // 5 (2D) or 16 (3D) arrays of npad floats
+    int box_total;     // floats of the child-group blocks
+    const int *off;    // [8]: float offset of the height-h child groups
+    const float *box;  // child-group blocks of (3*dim+2) x 32 floats
+    const float *prim; // cluster blocks of 5 (2D) or 16 (3D) x 32 floats
     const int *wide2bin;
 };
 
@@ -52,23 +55,24 @@ __device__ __forceinline__ unsigned order_key(float d, unsigned lane) {
 // Squared lower bound of the distance from p to the primitives of a node: the
 // larger of the box distance and the distance outside the node's slab
 // {x : |n.x - c| <= h}.
+// Children of node `parent` at height h+1 (so the children have height h).
 template <int DIM>
-__device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int idx, float px,
+__device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int parent, float px,
                                                float py, float pz) {
-    const int t = w.box_total;
-    const float *b = w.box + w.off[h] + idx;
-    const float lx = b[0], ly = b[t];
+    constexpr int NB = 3 * DIM + 2;
+    const float *b = w.box + w.off[h] + parent * (NB * 32) + (threadIdx.x & 31u);
+    const float lx = b[0], ly = b[32];
     float dx, dy;
     if (DIM == 2) {
-        const float hx = b[2 * t], hy = b[3 * t];
-        const float nx = b[4 * t], ny = b[5 * t], c = b[6 * t], th = b[7 * t];
+        const float hx = b[64], hy = b[96];
+        const float nx = b[128], ny = b[160], c = b[192], th = b[224];
         dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
         dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
         const float ds = fmaxf(0.0f, fabsf(nx * px + ny * py - c) - th);
         return fmaxf(dx * dx + dy * dy, ds * ds);
     }
-    const float lz = b[2 * t], hx = b[3 * t], hy = b[4 * t], hz = b[5 * t];
-    const float nx = b[6 * t], ny = b[7 * t], nz = b[8 * t], c = b[9 * t], th = b[10 * t];
+    const float lz = b[64], hx = b[96], hy = b[128], hz = b[160];
+    const float nx = b[192], ny = b[224], nz = b[256], c = b[288], th = b[320];
     dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
     dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
     const float dz = fmaxf(0.0f, fmaxf(lz - pz, pz - hz));
@@ -76,13 +80,14 @@ __device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int idx
     return fmaxf(dx * dx + dy * dy + dz * dz, ds * ds);
 }
 
+// Primitive of this lane in leaf cluster `cluster`.
 template <int DIM>
-__device__ __forceinline__ float wide_prim_dist(const WideView &w, int s, float px, float py,
-                                                float pz) {
-    const int np = w.npad;
-    const float *r = w.prim + s;
+__device__ __forceinline__ float wide_prim_dist(const WideView &w, int cluster, float px,
+                                                float py, float pz) {
+    constexpr int NF = DIM == 2 ? 5 : 16;
+    const float *r = w.prim + cluster * (NF * 32) + (threadIdx.x & 31u);
     if (DIM == 2) {
-        const float x0 = r[0], y0 = r[np], vx = r[2 * np], vy = r[3 * np], inv = r[4 * np];
+        const float x0 = r[0], y0 = r[32], vx = r[64], vy = r[96], inv = r[128];
         const float wx = px - x0, wy = py - y0;
         const float t = fminf(fmaxf((wx * vx + wy * vy) * inv, 0.0f), 1.0f);
         const float dx = wx - t * vx, dy = wy - t * vy;
@@ -91,7 +96,7 @@ __device__ __forceinline__ float wide_prim_dist(const WideView &w, int s, float 
     float4 rec[4];
     float *f = reinterpret_cast<float *>(rec);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) f[k] = r[k * np];
+    for (int k = 0; k < 16; ++k) f[k] = r[k * 32];
     return eberly32(px, py, pz, rec);
 }
 
@@ -105,8 +110,7 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
     float best = INFINITY, limit = INFINITY;
     int slot = -1;
     auto leaf = [&](int cluster) {
-        const int s = cluster * 32 + static_cast<int>(lane);
-        const float d2 = wide_prim_dist<DIM>(w, s, px, py, pz);
+        const float d2 = wide_prim_dist<DIM>(w, cluster, px, py, pz);
         const unsigned u = __reduce_min_sync(kAll, __float_as_uint(d2));
         const float m = __uint_as_float(u);
         if (m < best) {
@@ -115,13 +119,30 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
             limit = best > exact2 ? best * keep : best;
         }
     };
+    auto take_nearest = [&](unsigned &m, float d) -> unsigned {
+        const unsigned key = ((m >> lane) & 1u) ? order_key(d, lane) : 0xffffffffu;
+        const unsigned k = __reduce_min_sync(kAll, key) & 31u;
+        m &= ~(1u << k);
+        return k;
+    };
     if (w.H == 1) {
         leaf(0);
         return WideResult{best, slot};
     }
+    if (w.H == 2) {
+        // root children are the leaf clusters: visit them nearest first
+        const float d = wide_box_dist<DIM>(w, 1, 0, px, py, pz);
+        unsigned m = __ballot_sync(kAll, d < limit);
+        while (m) {
+            const unsigned k = take_nearest(m, d);
+            leaf(static_cast<int>(k));
+            m &= __ballot_sync(kAll, d < limit);
+        }
+        return WideResult{best, slot};
+    }
     int h = w.H;    // height of the current node
     int node = 0;   // its index at that height
-    float d = wide_box_dist<DIM>(w, h - 1, static_cast<int>(lane), px, py, pz);
+    float d = wide_box_dist<DIM>(w, h - 1, node, px, py, pz);
     unsigned m = __ballot_sync(kAll, d < limit);
     for (;;) {
         if (m == 0u) {
@@ -130,15 +151,13 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
             const unsigned left = static_cast<unsigned>(node) & 31u;
             node >>= 5;
             ++h;
-            d = wide_box_dist<DIM>(w, h - 1, node * 32 + static_cast<int>(lane), px, py, pz);
+            d = wide_box_dist<DIM>(w, h - 1, node, px, py, pz);
             const unsigned key = order_key(d, lane);
             const unsigned key_left = __shfl_sync(kAll, key, left);
             m = __ballot_sync(kAll, key > key_left && d < limit);
             continue;
         }
-        const unsigned key = ((m >> lane) & 1u) ? order_key(d, lane) : 0xffffffffu;
-        const unsigned k = __reduce_min_sync(kAll, key) & 31u;
-        m &= ~(1u << k);
+        const unsigned k = take_nearest(m, d);
         const int child = node * 32 + static_cast<int>(k);
         if (h == 2) {
             leaf(child);
@@ -146,7 +165,7 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         } else {
             node = child;
             --h;
-            d = wide_box_dist<DIM>(w, h - 1, node * 32 + static_cast<int>(lane), px, py, pz);
+            d = wide_box_dist<DIM>(w, h - 1, node, px, py, pz);
             m = __ballot_sync(kAll, d < limit);
         }
     }

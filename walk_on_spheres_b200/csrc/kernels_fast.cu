@@ -456,7 +456,7 @@ FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, in
     p.chunks = (n_walks + p.chunk - 1) / p.chunk;
     p.n_tasks = n_points * p.chunks;
     // stage the wide boxes, and the primitives too when they fit, in shared memory
-    const size_t box_floats = static_cast<size_t>(3 * w.dim + 2) * w.box_total;
+    const size_t box_floats = static_cast<size_t>(w.box_total);
     const size_t prim_floats = static_cast<size_t>(w.dim == 2 ? 5 : 16) * w.npad;
     const size_t cap = std::min<size_t>(96 * 1024, smem_optin);
     p.stage_scene = precision == 32 && box_floats * 4 <= cap;
@@ -490,7 +490,7 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
     a.n_tasks = plan.n_tasks;
     a.w = w;
     a.stage = plan.stage_scene ? 1 : 0;
-    a.stage_box = plan.stage_scene ? (3 * w.dim + 2) * w.box_total : 0;
+    a.stage_box = plan.stage_scene ? w.box_total : 0;
     a.stage_prim = plan.stage_prims ? (w.dim == 2 ? 5 : 16) * w.npad : 0;
     // FP32 queries are conservative to a relative tau = 2^-10 outside the
     // epsilon shell and exact inside it (see Nearest32)

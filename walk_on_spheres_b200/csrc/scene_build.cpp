@@ -252,27 +252,31 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
             }
         }
     }
-    // heights 1..H-1 are children of some node: 32 * cnt[h+1] entries each
+    // heights 1..H-1 are children of some node.  Children of one parent form
+    // a group block of nbox x 32 floats (field f of child k at f*32 + k):
+    // box lo[dim], hi[dim], slab normal[dim], slab offset, half-thickness.
+    const int nbox = nc + dim + 2;
     int total = 0;
     for (int h = 1; h < H; ++h) {
         sc.w_off[h] = total;
-        total += static_cast<int>(32 * cnt[h + 1]);
+        total += static_cast<int>(cnt[h + 1]) * nbox * 32;
     }
-    sc.w_box_total = std::max(total, 32);
+    sc.w_box_total = std::max(total, nbox * 32);
     const double widen = std::ldexp(sc.scale, -20);
-    // per node: box lo[dim], hi[dim], then slab normal n[dim], offset c and
-    // half-thickness h (all SoA)
-    const int nbox = nc + dim + 2;
-    sc.wbox.assign(static_cast<size_t>(nbox) * sc.w_box_total, 0.0f);
-    for (int c = 0; c < nbox; ++c) {
-        float *arr = sc.wbox.data() + static_cast<size_t>(c) * sc.w_box_total;
-        // padding boxes are empty (lo = +inf, hi = -inf): infinitely far;
-        // their slab is unbounded (h = +inf)
-        float fill = 0.0f;
-        if (c < dim) fill = INFINITY;
-        else if (c < nc) fill = -INFINITY;
-        else if (c == nbox - 1) fill = INFINITY;
-        for (int i = 0; i < sc.w_box_total; ++i) arr[i] = fill;
+    sc.wbox.assign(static_cast<size_t>(sc.w_box_total), 0.0f);
+    // padding children are empty boxes (lo = +inf, hi = -inf) with an
+    // unbounded slab: infinitely far
+    for (int h = 1; h < H; ++h) {
+        for (long long g = 0; g < cnt[h + 1]; ++g) {
+            float *blk = sc.wbox.data() + sc.w_off[h] + static_cast<size_t>(g) * nbox * 32;
+            for (int f = 0; f < nbox; ++f) {
+                float fill = 0.0f;
+                if (f < dim) fill = INFINITY;
+                else if (f < nc) fill = -INFINITY;
+                else if (f == nbox - 1) fill = INFINITY;
+                for (int k = 0; k < 32; ++k) blk[f * 32 + k] = fill;
+            }
+        }
     }
     auto vertex = [&](int prim, int j, double *out) {
         const int v = sc.prims[static_cast<size_t>(dim) * prim + j];
@@ -283,10 +287,11 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
         long long span_h = 1;
         for (int k = 0; k < h; ++k) span_h *= 32;
         for (long long i = 0; i < cnt[h]; ++i) {
+            float *blk = sc.wbox.data() + sc.w_off[h] + static_cast<size_t>(i / 32) * nbox * 32;
+            const int lane = static_cast<int>(i % 32);
             for (int k = 0; k < nc; ++k) {
                 const double v = lv[h][static_cast<size_t>(i) * nc + k];
-                sc.wbox[static_cast<size_t>(k) * sc.w_box_total + sc.w_off[h] + i] =
-                    k < dim ? round_down(v - widen) : round_up(v + widen);
+                blk[k * 32 + lane] = k < dim ? round_down(v - widen) : round_up(v + widen);
             }
             // slab of every vertex of the node's primitives
             pts.clear();
@@ -311,17 +316,16 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
                 for (int k = 0; k < dim; ++k) t += static_cast<double>(nf[k]) * pts[q * dim + k];
                 t32 = std::max(t32, std::fabs(t));
             }
-            const size_t at = static_cast<size_t>(sc.w_off[h] + i);
-            for (int k = 0; k < dim; ++k) sc.wbox[static_cast<size_t>(nc + k) * sc.w_box_total + at] = nf[k];
-            sc.wbox[static_cast<size_t>(nc + dim) * sc.w_box_total + at] = cf;
-            sc.wbox[static_cast<size_t>(nc + dim + 1) * sc.w_box_total + at] =
-                round_up(t32 + 4.0 * widen);
+            for (int k = 0; k < dim; ++k) blk[(nc + k) * 32 + lane] = nf[k];
+            blk[(nc + dim) * 32 + lane] = cf;
+            blk[(nc + dim + 1) * 32 + lane] = round_up(t32 + 4.0 * widen);
         }
     }
-    // primitive SoA in wide-slot order; padding primitives are far away
+    // primitives in wide-slot order, one block of na x 32 floats per cluster
+    // (field f of slot 32c + k at c*na*32 + f*32 + k); padding primitives are
+    // far away
     const int na = dim == 2 ? 5 : 16;
-    const size_t np = static_cast<size_t>(sc.w_npad);
-    sc.wprim.assign(np * na, 0.0f);
+    sc.wprim.assign(static_cast<size_t>(sc.w_npad) * na, 0.0f);
     for (int s = 0; s < sc.w_npad; ++s) {
         float rec[16];
         if (s >= n) {
@@ -336,7 +340,8 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
             const int b = sc.wide2bin[s];
             for (int k = 0; k < 16; ++k) rec[k] = sc.tri32[16 * static_cast<size_t>(b) + k];
         }
-        for (int k = 0; k < na; ++k) sc.wprim[static_cast<size_t>(k) * np + s] = rec[k];
+        float *blk = sc.wprim.data() + static_cast<size_t>(s / 32) * na * 32;
+        for (int k = 0; k < na; ++k) blk[k * 32 + s % 32] = rec[k];
     }
 }
 
