@@ -158,6 +158,22 @@ int wos_solve_grid_device(wos_context *ctx, const wos_params *params, const wos_
                           double *mean, double *variance, double *standard_error,
                           double *mean_steps, uint8_t *location, wos_counters *counters);
 
+/* As wos_solve_grid_device, but allocating no device memory; it has no
+ * counterpart in the reference.  For callers that cannot call cudaMalloc
+ * while they solve (an allocator or pool that owns the device budget, code
+ * that must not synchronise the device, hosts that forbid allocation after
+ * start-up).  Temporaries live in one static 8 MiB device array inside the
+ * library, so grids are limited to 103 000 points (WOS_ERR_INVALID beyond);
+ * the FAST methods run one walk task per point.  The first call on a device
+ * looks up the array's device address (call it once before any stream
+ * capture); calls that overlap on the GPU share the array and race, so
+ * serialise them.  The context (mesh upload) is set up by the allocating
+ * entry points beforehand. */
+int wos_solve_grid_device_noalloc(wos_context *ctx, const wos_params *params,
+                                  const wos_grid *grid, double *mean, double *variance,
+                                  double *standard_error, double *mean_steps, uint8_t *location,
+                                  wos_counters *counters);
+
 /* The point-level operator: wos_run (include/wos/wos.hpp:160-191) with
  * get_start_point (wos.hpp:42-52) and classification for `n` arbitrary start
  * points (host array n*dim).  point_index[i] plays the role of the grid

@@ -41,6 +41,7 @@ CUDA_UNITS = {
     "kernels_fast.cu": [],
     # host code that includes the device headers' type definitions
     "context.cpp": ["-x", "cu"],
+    "noalloc.cu": [],
 }
 HOST_UNITS = ["scene_build.cpp", "obj_reader.cpp", "runner.cpp", "h5_writer.cpp", "host_api.cpp"]
 CLI_UNITS = ["cli_main.cpp"]
