@@ -57,7 +57,10 @@ UNIT = "walks/s"
 # the workload's walks, times the reference record sizes (40 B node, 40 B
 # segment); measured by `python -m oracle.measure_traversal`.
 BYTES_PER_QUERY = 1863.4
-TRAFFIC_FILE = ROOT / "profiles" / "roofline_traffic.json"
+# DRAM bytes (read + write) of one walk-kernel launch of this workload, from a
+# one-pass ncu capture of the full launch (profiles/walk_fast_kernel_poisson2d_
+# circle1024.md): 2.84 MB and 3.32 MB for the two source modes.
+TRAFFIC_BYTES_PER_LAUNCH = 3.08e6
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -167,14 +170,6 @@ def hbm_peak():
         return float(p["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (burst copy), of measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s, of fallback"
-
-
-def traffic_per_launch():
-    try:
-        t = json.loads(TRAFFIC_FILE.read_text())
-        return t.get(WORKLOAD)
-    except Exception:
-        return None
 
 
 # ---------------------------------------------------------------- CPU reference
@@ -363,7 +358,7 @@ def gpu_arm(args, rank, world, local):
     avg_kernel_s = (sum(kernel_ms) / len(kernel_ms)) / 1000.0
     queries_per_launch = steps_total / len(kernel_ms)
     achieved = BYTES_PER_QUERY * queries_per_launch / avg_kernel_s / 1e9
-    traffic = traffic_per_launch()
+    traffic = TRAFFIC_BYTES_PER_LAUNCH if args.method == "fast" and args.walks == N_WALKS else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
