@@ -132,3 +132,30 @@ def test_solve_points_matches_grid(solver):
     assert np.array_equal(r.location, g.location.ravel())
     ins = r.location == 1
     assert np.array_equal(r.mean[ins], g.mean.ravel()[ins])
+
+
+def test_sharded_solver_matches_grid(solver):
+    """The per-shard GPU solver (walk_on_spheres_b200.parallel) reproduces the
+    grid sweep point for point: same coordinates, same global-index seeds."""
+    import os
+    import socket
+    import torch.distributed as dist
+    from walk_on_spheres_b200 import parallel
+    solver.set_mesh(mesh_by_name("annulus"))
+    grid = solver.grid_over_mesh(20, 18, 1)
+    g = solver.solve_grid("laplace", grid=grid, N_walks=200, seed=3, method="fast")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        out = parallel.solve_grid_sharded(
+            parallel.gpu_shard_solver(solver, "laplace", grid, N_walks=200, seed=3, method="fast"),
+            parallel.grid_size(grid, 2))
+    finally:
+        dist.destroy_process_group()
+    assert np.array_equal(out["location"], g.location.ravel())
+    ins = out["location"] == 1
+    assert np.allclose(out["mean"][ins], g.mean.ravel()[ins], rtol=1e-12, atol=1e-14)

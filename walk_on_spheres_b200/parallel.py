@@ -1,0 +1,111 @@
+"""Sharding one grid sweep across processes (one per GPU) with torch.distributed.
+
+The reference splits the grid into MPI blocks (include/wos/runner.hpp:90-134);
+because every point is seeded from its global linear index
+(runner.hpp:163-168) the fields do not depend on the split (README.md:87-90).
+Here rank r solves the contiguous linear-index range
+[n*r/world, n*(r+1)/world) of the grid — its own points, seeded by their
+global index — and rank 0 gathers the fields and sums the counters, the
+counterpart of runner.hpp:240-263 and of the collective HDF5 write.  There
+is no collective inside the walk loop; the only communication is one gather
+of the fields and one reduction of a few scalars at the end.
+
+    import torch.distributed as dist
+    from walk_on_spheres_b200 import Solver, meshes, parallel
+    dist.init_process_group("nccl")
+    s = Solver(local_rank).set_mesh(meshes.circle())
+    grid = s.grid_over_mesh(256, 256)
+    out = parallel.solve_grid_sharded(parallel.gpu_shard_solver(s, "poisson", grid, N_walks=4096,
+                                      seed=1), parallel.grid_size(grid, s.dim))
+    # rank 0: out["mean"] etc. are the full (Nx*Ny*Nz,) fields
+"""
+from __future__ import annotations
+
+import numpy as np
+
+FIELDS = ("mean", "variance", "standard_error", "mean_steps", "location")
+COUNTS = ("inside_points", "max_steps_hits", "ambiguous_ray_retries", "indeterminate_points",
+          "total_walks", "total_steps")
+
+
+def grid_size(grid, dim: int) -> int:
+    return int(grid.Nx) * int(grid.Ny) * (int(grid.Nz) if dim == 3 else 1)
+
+
+def shard_bounds(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous linear-index range of `rank` (sizes differ by at most one)."""
+    return n * rank // world, n * (rank + 1) // world
+
+
+def grid_points(grid, dim: int, start: int, end: int) -> np.ndarray:
+    """Coordinates of linear indices [start, end) of `grid`, computed like
+    grid_coordinate (include/wos/grid.hpp:12-18): min + (max-min)*i/(N-1)."""
+    nx, ny = int(grid.Nx), int(grid.Ny)
+    nz = int(grid.Nz) if dim == 3 else 1
+    lin = np.arange(start, end, dtype=np.int64)
+    i, j, k = lin // (ny * nz), (lin // nz) % ny, lin % nz
+
+    def coord(lo, hi, idx, count):
+        if count <= 1:
+            return np.full(idx.shape, lo, dtype=np.float64)
+        return lo + (hi - lo) * idx.astype(np.float64) / float(count - 1)
+
+    cols = [coord(grid.xmin, grid.xmax, i, nx), coord(grid.ymin, grid.ymax, j, ny)]
+    if dim == 3:
+        cols.append(coord(grid.zmin, grid.zmax, k, nz))
+    return np.stack(cols, axis=1)
+
+
+def gpu_shard_solver(solver, equation: str, grid, **params):
+    """Per-shard solve on this rank's GPU through wos_solve_points, each point
+    seeded by its global linear index."""
+
+    def solve(start: int, end: int) -> dict:
+        pts = grid_points(grid, solver.dim, start, end)
+        r = solver.solve_points(equation, pts, point_index=np.arange(start, end, dtype=np.uint64),
+                                **params)
+        out = {k: getattr(r, k) for k in FIELDS}
+        out["counters"] = r.counters
+        return out
+
+    return solve
+
+
+def solve_grid_sharded(solve_shard, n_points: int, group=None, device=None) -> dict | None:
+    """Solve this rank's shard with `solve_shard(start, end)` and gather the full
+    fields on rank 0 (other ranks return None).  `device` is where the
+    collective tensors live (a CUDA device for NCCL, None / "cpu" for gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    rank = dist.get_rank(group)
+    world = dist.get_world_size(group)
+    start, end = shard_bounds(n_points, rank, world)
+    local = solve_shard(start, end)
+    m = end - start
+    width = -(-n_points // world) + 1          # longest shard
+    buf = np.full((len(FIELDS), width), np.nan)
+    for f, name in enumerate(FIELDS):
+        buf[f, :m] = np.asarray(local[name], dtype=np.float64)[:m]
+    t = torch.from_numpy(buf)
+    c = local.get("counters", {})
+    counts = torch.tensor([float(c.get(k, 0)) for k in COUNTS], dtype=torch.float64)
+    times = torch.tensor([float(c.get("total_ms", 0.0))], dtype=torch.float64)
+    if device is not None and str(device) != "cpu":
+        t, counts, times = t.to(device), counts.to(device), times.to(device)
+    gathered = [torch.empty_like(t) for _ in range(world)] if rank == 0 else None
+    dist.gather(t, gathered, dst=0, group=group)
+    dist.all_reduce(counts, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(times, op=dist.ReduceOp.MAX, group=group)
+    if rank != 0:
+        return None
+    out = {}
+    for f, name in enumerate(FIELDS):
+        full = np.empty(n_points, dtype=np.float64)
+        for r in range(world):
+            s, e = shard_bounds(n_points, r, world)
+            full[s:e] = gathered[r][f, :e - s].cpu().numpy()
+        out[name] = full.astype(np.uint8) if name == "location" else full
+    out["counters"] = {k: int(v) for k, v in zip(COUNTS, counts.cpu().tolist())}
+    out["counters"]["total_ms_max_over_ranks"] = float(times.item())
+    return out
