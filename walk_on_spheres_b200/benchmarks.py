@@ -1,0 +1,135 @@
+"""Throughput and accuracy of the single-solve workloads, per walk method.
+
+    python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0]
+
+Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
+
+* laplace2d_annulus256_64sq — `laplace` on the annulus 0.5 < r < 1
+  (2 x 128 segments), 64 x 64 grid, 10 000 walks, eps 0.01, seed 12345;
+  analytic u = (16/15 r^2 - 1/(15 r^2)) cos 2 theta.
+* poisson2d_circle1024_256sq_{uniform,green} — `poisson` on the unit circle
+  (1024 segments), 256 x 256 grid, 4096 walks; analytic piecewise solution of
+  the f = 0.1 disk load.
+* screened3d_sphere16128_64cube — `screened_poisson`, alpha 10, on the UV
+  sphere with 128 x 64 bands (16 128 triangles), 64^3 grid, 1024 walks,
+  seed 7 (eps clamped to 0.005).
+
+For each workload and method it prints device walks/s, closest-point
+queries/s, mean steps and, against PLAIN_FP64 (the reference estimator and
+streams), the mean |difference| / combined standard error and the variance
+ratio; where an analytic solution exists, the largest |mean - u| and the
+fraction of points within 5 SE + eps max|grad u|.  `--scale` multiplies the
+walk counts (e.g. 0.25 for a quick look); PLAIN_FP64 runs with at most 256
+walks per point on the 3D workload to keep it within a minute.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+
+import numpy as np
+
+from . import meshes
+from .solver import Solver
+
+
+def _annulus_u(X, Y, Z):
+    r2 = X * X + Y * Y
+    return (16.0 / 15.0 * r2 - 1.0 / (15.0 * r2)) * (X * X - Y * Y) / r2
+
+
+def _disk_u(X, Y, Z, f=0.1, a=0.15):
+    r = np.hypot(X, Y)
+    return np.where(r <= a, f / 4 * (a * a - r * r) + f * a * a / 2 * np.log(1 / a),
+                    f * a * a / 2 * np.log(1 / np.maximum(r, 1e-300)))
+
+
+WORKLOADS = {
+    "laplace2d_annulus256_64sq": dict(mesh=meshes.annulus, eq="laplace", grid=(64, 64, 1),
+                                      walks=10000, kw=dict(seed=12345), analytic=_annulus_u,
+                                      grad=2.2),
+    "poisson2d_circle1024_256sq_uniform": dict(
+        mesh=lambda: meshes.circle(segments=1024), eq="poisson", grid=(256, 256, 1), walks=4096,
+        kw=dict(seed=12345, source_mode="uniform"), analytic=_disk_u, grad=0.0075),
+    "poisson2d_circle1024_256sq_green": dict(
+        mesh=lambda: meshes.circle(segments=1024), eq="poisson", grid=(256, 256, 1), walks=4096,
+        kw=dict(seed=12345, source_mode="green"), analytic=_disk_u, grad=0.0075),
+    "screened3d_sphere16128_64cube": dict(mesh=meshes.uv_sphere, eq="screened_poisson",
+                                          grid=(64, 64, 64), walks=1024,
+                                          kw=dict(seed=7, alpha=10.0), analytic=None, grad=None,
+                                          plain_walks=256),
+}
+
+
+def _coords(s: Solver, nx, ny, nz):
+    b = s.bbox
+    ax = [np.array([lo + (hi - lo) * i / (n - 1) if n > 1 else lo for i in range(n)])
+          for lo, hi, n in ((b[0], b[1], nx), (b[2], b[3], ny), (b[4], b[5], nz))]
+    return np.meshgrid(*ax, indexing="ij")
+
+
+def run(name: str, scale: float = 1.0, device: int = 0) -> dict:
+    w = WORKLOADS[name]
+    s = Solver(device).set_mesh(w["mesh"]())
+    nx, ny, nz = w["grid"]
+    walks = max(16, int(round(w["walks"] * scale)))
+    out = {"workload": name, "walks": walks, "methods": {}}
+    res = {}
+    for method in ("fast", "fast64", "plain"):
+        n = walks if method != "plain" else min(walks, w.get("plain_walks", walks))
+        r = s.solve_grid(w["eq"], nx, ny, nz, N_walks=n, method=method, **w["kw"])
+        c = r.counters
+        secs = c["walk_ms"] / 1000.0
+        res[method] = r
+        ins = r.location == 1
+        out["methods"][method] = {
+            "walks": n,
+            "walks_per_s": c["total_walks"] / secs,
+            "queries_per_s": c["total_steps"] / secs,
+            "walk_ms": c["walk_ms"], "classify_ms": c["classify_ms"],
+            "mean_steps": float(np.mean(r.mean_steps[ins])),
+            "variance_per_walk": float(np.mean(r.variance[ins])),
+        }
+    ins = res["plain"].location == 1
+    for method in ("fast", "fast64"):
+        a, b = res[method], res["plain"]
+        se = np.sqrt(a.standard_error[ins] ** 2 + b.standard_error[ins] ** 2)
+        live = se > 0
+        z = np.abs(a.mean[ins] - b.mean[ins])[live] / se[live]
+        m = out["methods"][method]
+        m["vs_plain_mean_abs_z"] = float(z.mean())
+        m["vs_plain_frac_within_3se"] = float((z <= 3).mean())
+        m["variance_ratio_plain_over_method"] = (
+            out["methods"]["plain"]["variance_per_walk"] / m["variance_per_walk"])
+        m["matched_se_speedup_vs_plain"] = (
+            m["walks_per_s"] / out["methods"]["plain"]["walks_per_s"]
+            * m["variance_ratio_plain_over_method"])
+    if w["analytic"] is not None:
+        X, Y, Z = _coords(s, nx, ny, nz)
+        u = w["analytic"](X, Y, Z)
+        eps = res["plain"].counters["effective_epsilon"]
+        for method, r in res.items():
+            ins_m = r.location == 1
+            err = np.abs(r.mean - u)[ins_m]
+            bound = 5 * r.standard_error[ins_m] + eps * w["grad"] + 1e-6
+            out["methods"][method]["analytic_max_abs_err"] = float(err.max())
+            out["methods"][method]["analytic_frac_within_bound"] = float((err <= bound).mean())
+    s.close()
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--workloads", default=",".join(WORKLOADS))
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    for name in a.workloads.split(","):
+        print(json.dumps(run(name.strip(), a.scale, a.device)), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
