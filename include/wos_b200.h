@@ -183,6 +183,60 @@ int wos_solve_points(wos_context *ctx, const wos_params *params, const double *p
                      double *standard_error, double *mean_steps, uint8_t *location,
                      wos_counters *counters);
 
+/* ------------------------------------ Gaussian heat source and its adjoint */
+
+/* Source of the differentiable heat problem (no reference counterpart; the
+ * reference's only Gaussian source is the 2D welding one of
+ * apps/welding/include/welding/gaussian_heat_source.hpp, with another
+ * normalisation):
+ *     -Δu = f,  f(x) = Q exp(-|x - x0|^2 / sigma^2),
+ *     u = g on the boundary, g given per mesh vertex and interpolated at the
+ *     nearest boundary point (linearly along a segment in 2D,
+ *     barycentrically on a triangle in 3D). */
+typedef struct {
+    double Q;       /* amplitude */
+    double x0[3];   /* centre (x0[2] unused in 2D) */
+    double sigma;   /* width (> 0) */
+} wos_gaussian_source;
+
+/* Number of vertices of the current mesh (the length of the per-vertex
+ * boundary data). */
+int wos_mesh_vertex_count(const wos_context *ctx, int *n_verts);
+
+/* Forward solve at `n` probe points (host array n*dim) with the reference's
+ * Poisson walk estimator (include/wos/wos.hpp:54-138 with the Green kernels
+ * of include/wos/poisson.hpp:12-51) for the source above.  vertex_values:
+ * host array of n_verts boundary values (NULL: g = 0).  params: N_walks,
+ * epsilon (used as given), max_steps, max_ray_attempts, seed, source_mode
+ * (uniform / Green source samples) and method (FAST_FP32 or FAST_FP64;
+ * PLAIN_FP64 is rejected); params->equation and alpha are ignored.  Probe i
+ * is seeded like grid index point_index[i] (NULL: i).  Outputs as
+ * wos_solve_points (host arrays, any may be NULL); boundary probes get
+ * g(nearest), outside / indeterminate probes NaN. */
+int wos_heat_forward(wos_context *ctx, const wos_params *params,
+                     const wos_gaussian_source *source, const double *vertex_values,
+                     const double *probes, const uint64_t *point_index, long long n,
+                     double *mean, double *variance, double *standard_error,
+                     double *mean_steps, uint8_t *location, wos_counters *counters);
+
+/* Adjoint of wos_heat_forward for the same arguments: re-runs every walk
+ * from its seed (paths are not stored; the replayed values are bit-identical
+ * to the forward ones) and accumulates, for probe weights grad_u (host, n;
+ * dL/du_p; NULL: all 1):
+ *   grad_source[5]   sum_p grad_u[p] du_p/d(Q, x0.x, x0.y, x0.z, sigma)
+ *   grad_vertex_values[n_verts]   sum_p grad_u[p] du_p/dg_v
+ *   jacobian[n*5]    per-probe walk means of du_p/d(Q, x0.x, x0.y, x0.z, sigma)
+ *   jacobian_se[n*5] their standard errors
+ *   replayed_mean[n] the replayed probe values
+ * All host arrays; any may be NULL.  Outside / indeterminate probes carry NaN
+ * in jacobian and contribute nothing. */
+int wos_heat_adjoint(wos_context *ctx, const wos_params *params,
+                     const wos_gaussian_source *source, const double *vertex_values,
+                     const double *probes, const uint64_t *point_index, long long n,
+                     const double *grad_u, double *grad_source, double *grad_vertex_values,
+                     double *jacobian, double *jacobian_se, double *replayed_mean,
+                     wos_counters *counters);
+
 /* -------------------------------------------------- kernel-level checks */
 
 /* First `count` outputs of the device xoshiro256++ stream PRNG(seeds[s])

@@ -350,3 +350,40 @@ class Oracle(_Lib):
 
     def screened_epsilon(self, eps, alpha):
         return self._fn("screened_epsilon", C.c_double, [C.c_double, C.c_double])(eps, alpha)
+
+    def heat_solve(self, mesh, probes, Q: float, x0, sigma: float, vertex_values=None,
+                   weights=None, N_walks: int = 256, epsilon: float = 1e-3,
+                   max_steps: int = 10000, max_ray_attempts: int = 12, seed: int = 0,
+                   source_mode: int = 1, point_index=None, n_threads: int = 0) -> dict:
+        """FP64 Gaussian heat-source walks (wo_heat_solve): per-probe mean, standard error,
+        derivative means / standard errors du/d(Q, x0.x, x0.y, x0.z, sigma), locations and
+        grad_vertex = sum_i weights[i] du_i/dg_v."""
+        pts = np.ascontiguousarray(probes, dtype=np.float64).reshape(-1, mesh.dim)
+        n = pts.shape[0]
+        solve = Solve(mesh, 1, 1, 1, N_walks=N_walks, epsilon=epsilon, max_steps=max_steps,
+                      max_ray_attempts=max_ray_attempts, seed=seed, source_mode=source_mode,
+                      n_threads=n_threads,
+                      points=None if point_index is None else np.asarray(point_index))
+        pb, keep = self._problem(mesh, solve)
+        src = _Gaussian()
+        src.Q, src.sigma = float(Q), float(sigma)
+        xs = list(np.asarray(x0, dtype=np.float64).ravel()) + [0.0, 0.0, 0.0]
+        src.x0 = (C.c_double * 3)(*xs[:3])
+        g = None if vertex_values is None else np.ascontiguousarray(vertex_values, np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        out = {"mean": np.zeros(n), "standard_error": np.zeros(n),
+               "jacobian": np.zeros((n, 5)), "jacobian_se": np.zeros((n, 5)),
+               "location": np.zeros(n, dtype=np.uint8),
+               "grad_vertex": np.zeros(mesh.verts.shape[0])}
+        rc = self._fn("heat_solve", C.c_int, [C.POINTER(_Problem), C.POINTER(_Gaussian)] +
+                      [C.c_void_p] * 2 + [C.c_longlong] + [C.c_void_p] * 7)(
+            C.byref(pb), C.byref(src), _ptr(g), _ptr(pts), n, _ptr(w), _ptr(out["mean"]),
+            _ptr(out["standard_error"]), _ptr(out["jacobian"]), _ptr(out["jacobian_se"]),
+            _ptr(out["location"]), _ptr(out["grad_vertex"]))
+        if rc != 0:
+            raise RuntimeError(f"wo_heat_solve failed ({rc})")
+        return out
+
+
+class _Gaussian(C.Structure):
+    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double)]

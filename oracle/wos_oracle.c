@@ -416,6 +416,8 @@ typedef struct {
     double point[3];
     int prim;
     int bid;
+    int tri;    /* nearest primitive id in both dimensions (prim is -1 in 3D, as in
+                   the reference, whose 3D query returns no id) */
     long long pops, tests;
 } npq_result;
 
@@ -429,6 +431,7 @@ static npq_result bvh_npq(const bvh_t *t, const double p[3]) {
     r.point[0] = r.point[1] = r.point[2] = 0.0;
     r.prim = -1;
     r.bid = -1;
+    r.tri = -1;
     r.pops = r.tests = 0;
     int stack[64];
     int sp = 0;
@@ -456,6 +459,7 @@ static npq_result bvh_npq(const bvh_t *t, const double p[3]) {
                     r.point[0] = q[0];
                     r.point[1] = q[1];
                     r.point[2] = q[2];
+                    r.tri = t->prims[nd->idx + i];
                     if (d == 2) {
                         r.prim = prim;
                         r.bid = t->m.bids ? t->m.bids[prim] : 0;
@@ -1498,4 +1502,289 @@ int wo_walk_visit_counts(int equation_kind, const wo_problem *pb, int walks, lon
     *prim_tests = tally[2];
     *steps = tally[0];
     return rc;
+}
+
+/* ------------------------------------------------- Gaussian heat source */
+
+/* FP64 restatement of the heat-source walks and their derivative sums
+ * (walk_on_spheres_b200/csrc/kernels_adjoint.cu states the estimator).  The
+ * walk is the reference's Poisson estimator (include/wos/wos.hpp:54-138 with
+ * include/wos/poisson.hpp:12-51) on the reference's xoshiro256++ streams,
+ * seeded like the grid sweep (include/wos/runner.hpp:163-168, 208-221), with
+ * the source sampled at every step (no culling). */
+
+typedef struct {
+    const wo_problem *pb;
+    const wo_gaussian *src;
+    const bvh_t *t;
+    const double *g;
+    const double *probes;
+    long long n;
+    const double *weights;
+    double btol;
+    double *mean, *se, *jac, *jac_se;
+    unsigned char *location;
+    long long cursor;
+    pthread_mutex_t lock;
+} heat_job;
+
+typedef struct {
+    heat_job *job;
+    double *grad;  /* per-worker vertex gradient (n_verts) or NULL */
+} heat_worker;
+
+/* interpolation weights of primitive `prim` at its point q */
+static void heat_weights(const bvh_t *t, int prim, const double q[3], int v[3], double w[3]) {
+    const int d = t->m.dim;
+    for (int k = 0; k < 3; ++k) {
+        v[k] = k < d ? t->m.prims[d * prim + k] : 0;
+        w[k] = 0.0;
+    }
+    const vec3 a = vert(&t->m, v[0]), b = vert(&t->m, v[1]);
+    if (d == 2) {
+        const double vx = b.x - a.x, vy = b.y - a.y;
+        double s = ((q[0] - a.x) * vx + (q[1] - a.y) * vy) / (vx * vx + vy * vy);
+        s = s < 0.0 ? 0.0 : (s > 1.0 ? 1.0 : s);
+        w[0] = 1.0 - s;
+        w[1] = s;
+        return;
+    }
+    const vec3 c = vert(&t->m, v[2]);
+    const double e1[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
+    const double e2[3] = {c.x - a.x, c.y - a.y, c.z - a.z};
+    const double dd[3] = {q[0] - a.x, q[1] - a.y, q[2] - a.z};
+    const double A = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+    const double B = e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2];
+    const double C = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+    const double d1 = dd[0] * e1[0] + dd[1] * e1[1] + dd[2] * e1[2];
+    const double d2 = dd[0] * e2[0] + dd[1] * e2[1] + dd[2] * e2[2];
+    const double det = A * C - B * B;
+    double s = (C * d1 - B * d2) / det, u = (A * d2 - B * d1) / det;
+    if (s < 0.0) s = 0.0;
+    if (u < 0.0) u = 0.0;
+    if (s + u > 1.0) {
+        const double sum = s + u;
+        s /= sum;
+        u /= sum;
+    }
+    w[0] = 1.0 - s - u;
+    w[1] = s;
+    w[2] = u;
+}
+
+static double heat_boundary(const heat_job *job, int prim, const double q[3], double c,
+                            double *grad) {
+    int v[3];
+    double w[3];
+    heat_weights(job->t, prim, q, v, w);
+    double val = 0.0;
+    for (int k = 0; k < job->pb->dim; ++k) {
+        if (job->g) val += w[k] * job->g[v[k]];
+        if (grad && c != 0.0) grad[v[k]] += c * w[k];
+    }
+    return val;
+}
+
+/* one step's source term and its parameter derivatives (added to j) */
+static double heat_source(const heat_job *job, const double p[3], double R, xoshiro *rng,
+                          double j[5]) {
+    const int d = job->pb->dim;
+    const wo_gaussian *s = job->src;
+    double y[3] = {0.0, 0.0, 0.0};
+    double m;
+    if (job->pb->source_mode == 1) {
+        const double radius = d == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
+        if (d == 2) {
+            const double angle = 2.0 * M_PI * rng_unit(rng);
+            y[0] = p[0] + radius * cos(angle);
+            y[1] = p[1] + radius * sin(angle);
+        } else {
+            const double z = 2.0 * rng_unit(rng) - 1.0;
+            const double angle = 2.0 * M_PI * rng_unit(rng);
+            const double xy = sqrt(1.0 - z * z);
+            y[0] = p[0] + radius * xy * cos(angle);
+            y[1] = p[1] + radius * xy * sin(angle);
+            y[2] = p[2] + radius * z;
+        }
+        m = d == 2 ? pg_mass_2d(R) : pg_mass_3d(R);
+    } else {
+        if (d == 2) ball_2d(p, R, rng, y);
+        else ball_3d(p, R, rng, y);
+        double r = dist3(p, y, d);
+        if (r > R) r = R;
+        if (!(r > 0.0)) return 0.0;
+        const double vol = d == 2 ? M_PI * R * R : 4.0 * M_PI * (R * R * R) / 3.0;
+        m = vol * (d == 2 ? pg_green_2d(R, r) : pg_green_3d(R, r));
+    }
+    const double dx = y[0] - s->x0[0], dy = y[1] - s->x0[1];
+    const double dz = d == 3 ? y[2] - s->x0[2] : 0.0;
+    const double inv_s2 = 1.0 / (s->sigma * s->sigma);
+    const double q = (dx * dx + dy * dy + dz * dz) * inv_s2;
+    const double e = exp(-q);
+    const double mf = m * s->Q * e;
+    j[0] += m * e;
+    j[1] += 2.0 * mf * inv_s2 * dx;
+    j[2] += 2.0 * mf * inv_s2 * dy;
+    j[3] += 2.0 * mf * inv_s2 * dz;
+    j[4] += 2.0 * mf * q / s->sigma;
+    return mf;
+}
+
+static void heat_probe(heat_worker *wk, long long i) {
+    heat_job *job = wk->job;
+    const wo_problem *pb = job->pb;
+    const int d = pb->dim;
+    double p0[3] = {job->probes[d * i], job->probes[d * i + 1],
+                    d == 3 ? job->probes[d * i + 2] : 0.0};
+    const uint64_t linear = pb->points ? (uint64_t)pb->points[i] : (uint64_t)i;
+    const uint64_t point_seed = wo_splitmix64(pb->seed ^ wo_splitmix64(linear));
+    const npq_result s0 = bvh_npq(job->t, p0);
+    int where;
+    if (d == 2) {
+        if (s0.dist <= job->btol) {
+            where = 2;
+        } else {
+            mesh_view m = {2, pb->n_prims, pb->verts, pb->prims, pb->boundary_ids};
+            where = winding_number(&m, p0) != 0 ? 1 : 0;
+        }
+    } else {
+        xoshiro ins;
+        rng_seed(&ins, wo_splitmix64(point_seed ^ 0x243F6A8885A308D3ULL));
+        int retries = 0;
+        where = classify_3d(job->t, p0, s0.dist, job->btol, pb->max_ray_attempts, &ins, &retries);
+    }
+    double mean = NAN, se = NAN, jm[5], js[5];
+    for (int k = 0; k < 5; ++k) jm[k] = js[k] = NAN;
+    const double wgt = job->weights ? job->weights[i] : 1.0;
+    if (where == 2) {
+        mean = heat_boundary(job, s0.tri, s0.point, wgt, wk->grad);
+        se = 0.0;
+        for (int k = 0; k < 5; ++k) jm[k] = js[k] = 0.0;
+    } else if (where == 1) {
+        xoshiro walk, srcr;
+        rng_seed(&walk, wo_splitmix64(point_seed ^ 0x13198A2E03707344ULL));
+        rng_seed(&srcr, wo_splitmix64(point_seed ^ 0xA4093822299F31D0ULL));
+        xoshiro *src = d == 2 ? &srcr : &walk;
+        const int N = pb->N_walks;
+        const double c = wgt / (double)N;
+        double m = 0.0, m2 = 0.0, sum[5] = {0, 0, 0, 0, 0}, sq[5] = {0, 0, 0, 0, 0};
+        for (int w = 0; w < N; ++w) {
+            double p[3] = {p0[0], p0[1], p0[2]};
+            double np[3] = {s0.point[0], s0.point[1], s0.point[2]};
+            int tri = s0.tri;
+            double R = s0.dist, sample = 0.0, j[5] = {0, 0, 0, 0, 0};
+            int steps = 0;
+            while (R > pb->epsilon && steps < pb->max_steps) {
+                sample += heat_source(job, p, R, src, j);
+                double q[3];
+                if (d == 2) step_2d(p, R, &walk, q);
+                else step_3d(p, R, &walk, q);
+                p[0] = q[0];
+                p[1] = q[1];
+                p[2] = q[2];
+                ++steps;
+                const npq_result r = bvh_npq(job->t, p);
+                R = r.dist;
+                np[0] = r.point[0];
+                np[1] = r.point[1];
+                np[2] = r.point[2];
+                tri = r.tri;
+            }
+            const double value = sample + heat_boundary(job, tri, np, c, wk->grad);
+            const double before = value - m;
+            m += before / (double)(w + 1);
+            m2 += before * (value - m);
+            for (int k = 0; k < 5; ++k) {
+                sum[k] += j[k];
+                sq[k] += j[k] * j[k];
+            }
+        }
+        mean = m;
+        const double var = N > 1 ? m2 / (double)(N - 1) : 0.0;
+        se = sqrt(var / (double)N);
+        for (int k = 0; k < 5; ++k) {
+            jm[k] = sum[k] / (double)N;
+            double v = N > 1 ? (sq[k] - sum[k] * jm[k]) / (double)(N - 1) : 0.0;
+            if (v < 0.0) v = 0.0;
+            js[k] = sqrt(v / (double)N);
+        }
+    }
+    if (job->mean) job->mean[i] = mean;
+    if (job->se) job->se[i] = se;
+    if (job->location) job->location[i] = (unsigned char)where;
+    for (int k = 0; k < 5; ++k) {
+        if (job->jac) job->jac[5 * i + k] = jm[k];
+        if (job->jac_se) job->jac_se[5 * i + k] = js[k];
+    }
+}
+
+static void *heat_thread(void *arg) {
+    heat_worker *wk = (heat_worker *)arg;
+    heat_job *job = wk->job;
+    for (;;) {
+        pthread_mutex_lock(&job->lock);
+        const long long i = job->cursor++;
+        pthread_mutex_unlock(&job->lock);
+        if (i >= job->n) break;
+        heat_probe(wk, i);
+    }
+    return NULL;
+}
+
+int wo_heat_solve(const wo_problem *pb, const wo_gaussian *src, const double *vertex_values,
+                  const double *probes, long long n, const double *weights, double *mean,
+                  double *standard_error, double *jacobian, double *jacobian_se,
+                  unsigned char *location, double *grad_vertex) {
+    if (pb->dim != 2 && pb->dim != 3) return 1;
+    if (!(src->sigma > 0.0)) return 1;
+    bvh_t t;
+    bvh_build(&t, pb);
+    heat_job job;
+    memset(&job, 0, sizeof(job));
+    job.pb = pb;
+    job.src = src;
+    job.t = &t;
+    job.g = vertex_values;
+    job.probes = probes;
+    job.n = n;
+    job.weights = weights;
+    job.mean = mean;
+    job.se = standard_error;
+    job.jac = jacobian;
+    job.jac_se = jacobian_se;
+    job.location = location;
+    double box[6];
+    mesh_bbox(pb, box);
+    double scale = 1.0; /* runner.hpp:86-88 */
+    for (int k = 0; k < pb->dim; ++k) {
+        const double ext = box[2 * k + 1] - box[2 * k];
+        if (ext > scale) scale = ext;
+    }
+    job.btol = 1e-10 * scale;
+    pthread_mutex_init(&job.lock, NULL);
+    const int threads = pb->n_threads > 0 ? pb->n_threads : 1;
+    heat_worker *wk = (heat_worker *)calloc((size_t)threads, sizeof(heat_worker));
+    pthread_t *th = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int i = 0; i < threads; ++i) {
+        wk[i].job = &job;
+        wk[i].grad = grad_vertex ? (double *)calloc((size_t)pb->n_verts, sizeof(double)) : NULL;
+    }
+    if (threads == 1) {
+        heat_thread(&wk[0]);
+    } else {
+        for (int i = 0; i < threads; ++i) pthread_create(&th[i], NULL, heat_thread, &wk[i]);
+        for (int i = 0; i < threads; ++i) pthread_join(th[i], NULL);
+    }
+    if (grad_vertex) {
+        for (int v = 0; v < pb->n_verts; ++v) grad_vertex[v] = 0.0;
+        for (int i = 0; i < threads; ++i) {
+            for (int v = 0; v < pb->n_verts; ++v) grad_vertex[v] += wk[i].grad[v];
+            free(wk[i].grad);
+        }
+    }
+    pthread_mutex_destroy(&job.lock);
+    free(wk);
+    free(th);
+    bvh_free(&t);
+    return 0;
 }

@@ -109,6 +109,26 @@ double wo_screened_epsilon(double requested, double alpha);
 int wo_walk_visit_counts(int equation, const wo_problem *pb, int walks, long long *queries,
                          long long *node_pops, long long *prim_tests, long long *steps);
 
+/* Gaussian heat source (same layout as wos_gaussian_source in include/wos_b200.h). */
+typedef struct {
+    double Q;
+    double x0[3];
+    double sigma;
+} wo_gaussian;
+
+/* FP64 heat-source walks at `n` probes (host n*dim; probe i seeded like grid
+ * index pb->points[i], or i when pb->points is NULL): per probe the mean
+ * value and its standard error, the walk means of du/d(Q, x0.x, x0.y, x0.z,
+ * sigma) and their standard errors (n*5), the location code, and
+ * grad_vertex[v] = sum_i weights[i] du_i/dg_v (weights NULL: all 1).  Uses
+ * pb's mesh, N_walks, epsilon, max_steps, max_ray_attempts, seed,
+ * source_mode and n_threads.  Any output may be NULL.  Returns 0 on
+ * success. */
+int wo_heat_solve(const wo_problem *pb, const wo_gaussian *src, const double *vertex_values,
+                  const double *probes, long long n, const double *weights, double *mean,
+                  double *standard_error, double *jacobian, double *jacobian_se,
+                  unsigned char *location, double *grad_vertex);
+
 #ifdef __cplusplus
 }
 #endif

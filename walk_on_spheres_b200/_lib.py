@@ -51,6 +51,11 @@ class Counters(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class GaussianSource(C.Structure):
+    """wos_gaussian_source: f(x) = Q exp(-|x - x0|^2 / sigma^2)."""
+    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double)]
+
+
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
                      C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double,
                      C.c_int)
@@ -82,6 +87,11 @@ SIGNATURES = {
     "wos_prng_u64": (C.c_int, [VP, VP, C.c_longlong, C.c_int, VP]),
     "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
+    "wos_heat_forward": (C.c_int, [VP, C.POINTER(Params), C.POINTER(GaussianSource), VP, VP, VP,
+                                   C.c_longlong] + [VP] * 5 + [C.POINTER(Counters)]),
+    "wos_heat_adjoint": (C.c_int, [VP, C.POINTER(Params), C.POINTER(GaussianSource), VP, VP, VP,
+                                   C.c_longlong] + [VP] * 6 + [C.POINTER(Counters)]),
     "wos_build_wide_bvh": (C.c_int, [C.c_int, VP, C.c_int, VP, C.c_int] + [VP] * 5),
     "wos_equation_registry": (C.POINTER(EquationEntry), [C.POINTER(C.c_int)]),
     "wos_peek_mesh_dim": (C.c_int, [C.c_char_p]),

@@ -39,8 +39,10 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-para
 CUDA_UNITS = {
     "kernels_exact.cu": ["--fmad=false"],
     "kernels_fast.cu": [],
+    "kernels_adjoint.cu": [],
     # host code that includes the device headers' type definitions
     "context.cpp": ["-x", "cu"],
+    "heat_api.cpp": ["-x", "cu"],
     "noalloc.cu": [],
 }
 HOST_UNITS = ["scene_build.cpp", "obj_reader.cpp", "runner.cpp", "h5_writer.cpp", "host_api.cpp"]

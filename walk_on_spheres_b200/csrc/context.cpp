@@ -18,27 +18,19 @@
 using namespace wosb;
 
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
 
-int fail(wos_context *ctx, int code, const std::string &msg) {
+int wosb::fail(wos_context *ctx, int code, const std::string &msg) {
     if (ctx) ctx->error = msg;
     g_error = msg;
     return code;
 }
 
-int cuda_fail(wos_context *ctx, cudaError_t e, const char *what) {
+int wosb::cuda_fail(wos_context *ctx, cudaError_t e, const char *what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(e);
     return fail(ctx, WOS_ERR_CUDA, m);
 }
-
-#define WOS_CUDA(ctx, call, what)                      \
-    do {                                               \
-        cudaError_t e_ = (call);                       \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
-    } while (0)
-
-}  // namespace
 
 // ------------------------------------------------------------- buffers
 
@@ -78,9 +70,10 @@ wos_context::~wos_context() {
 }
 
 std::vector<DeviceBuffer *> wos_context::all_buffers() {
-    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &wbox, &wprim, &wide2bin, &woff, &location, &start,
+    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &wbox, &wprim, &wide2bin, &woff, &slotv, &location, &start,
             &f_mean, &f_var, &f_se, &f_steps, &f_loc, &partials, &queue, &counters, &points,
-            &index, &scratch_a, &scratch_b, &scratch_c, &scratch_d};
+            &index, &scratch_a, &scratch_b, &scratch_c, &scratch_d, &h_values, &h_gradu,
+            &h_gradg, &h_grads, &h_jac, &h_jacse};
 }
 
 // ------------------------------------------------------------- context
@@ -155,6 +148,7 @@ int wos_context::upload_scene() {
     WOS_CUDA(this, upload(wbox, h.wbox, stream), "upload wide boxes");
     WOS_CUDA(this, upload(wprim, h.wprim, stream), "upload wide primitives");
     WOS_CUDA(this, upload(wide2bin, h.wide2bin, stream), "upload wide slot map");
+    WOS_CUDA(this, upload(slotv, h.slot_verts, stream), "upload slot vertex ids");
     WOS_CUDA(this, upload(woff, std::vector<int>(h.w_off, h.w_off + 8), stream),
              "upload wide offsets");
     WOS_CUDA(this, cudaStreamSynchronize(stream), "mesh upload");

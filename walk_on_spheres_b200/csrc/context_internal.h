@@ -21,7 +21,17 @@ struct DeviceBuffer {
 
 double effective_epsilon(const wos_params &p);
 
+// Records `msg` as the context's (and the thread's) last error; returns code.
+int fail(wos_context *ctx, int code, const std::string &msg);
+int cuda_fail(wos_context *ctx, cudaError_t e, const char *what);
+
 }  // namespace wosb
+
+#define WOS_CUDA(ctx, call, what)                                        \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) return ::wosb::cuda_fail(ctx, e_, what); \
+    } while (0)
 
 struct wos_context {
     int device = 0;
@@ -39,12 +49,14 @@ struct wos_context {
 
     // scene
     wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
-        wide2bin, woff;
+        wide2bin, woff, slotv;
     // per solve
     wosb::DeviceBuffer location, start, f_mean, f_var, f_se, f_steps, f_loc, partials, queue,
         counters, points, index;
     // kernel-level checks
     wosb::DeviceBuffer scratch_a, scratch_b, scratch_c, scratch_d;
+    // Gaussian heat source: vertex values, probe weights, gradients, Jacobian
+    wosb::DeviceBuffer h_values, h_gradu, h_gradg, h_grads, h_jac, h_jacse;
 
     // tuning overrides (<= 0: automatic)
     int chunk_override = 0;
@@ -54,6 +66,9 @@ struct wos_context {
     std::vector<wosb::DeviceBuffer *> all_buffers();
     int upload_scene();
     int run(const wos_params &p, const wosb::PointSet &ps, wosb::Fields out, wos_counters *c);
+    // Heat-source forward (h.adjoint == 0) or adjoint replay over `ps`.
+    int run_heat(const wos_params &p, const wosb::HeatDesc &h, const wosb::PointSet &ps,
+                 wosb::HeatOut out, wos_counters *c);
     int fields_for(long long n, wosb::Fields &out);
     int download(long long n, const wosb::Fields &dev, double *mean, double *variance, double *se,
                  double *steps, uint8_t *loc);

@@ -45,12 +45,14 @@ __device__ __forceinline__ void point_at(const PointSet &ps, long long t, double
 }
 
 // Start point of a point (include/wos/wos.hpp:35-52): nearest boundary point,
-// its distance and (2D) boundary id.  Written by the classification kernel.
+// its distance and (2D) boundary id, plus the binary-tree slot of the nearest
+// primitive (for per-vertex boundary data).  Written by the classification
+// kernel.
 struct StartRecord {
     double radius;
     double nx, ny, nz;
     int boundary_id;
-    int pad;
+    int slot;
 };
 
 // Equation selection for runtime dispatch.

@@ -60,6 +60,43 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
 FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, int n_walks,
                    int precision, int device_sms, size_t smem_optin);
 
+// Gaussian heat source -Δu = Q exp(-|x - x0|^2 / sigma^2) with per-vertex
+// Dirichlet data (kernels_adjoint.cu).
+struct HeatDesc {
+    int mode;               // kUniform / kGreen source sampling
+    double Q, x0[3], sigma;
+    const double *g;        // per-vertex boundary values (null: all zero)
+    const int *slot_verts;  // per binary-tree slot: the primitive's dim vertex ids
+    int adjoint;            // 0: forward walks; 1: replay accumulating derivatives
+    const double *grad_u;   // adjoint: weight of each point's value (dL/du_p)
+    double *grad_g;         // adjoint: dL/dg_v accumulators (zeroed by the caller)
+};
+
+// Per-task partial of the heat walks: value statistics as TaskPartial plus
+// sums and sums of squares of the five source-parameter derivatives
+// (Q, x0.x, x0.y, x0.z, sigma) in adjoint mode.
+struct HeatPartial {
+    double n, mean, m2, steps;
+    double jsum[5];
+    double jsq[5];
+    unsigned int hits;
+    unsigned int pad;
+};
+
+struct HeatOut {
+    Fields f;
+    double *jac;          // adjoint: n * 5 walk means of du_p/dtheta (optional)
+    double *jac_se;       // adjoint: their standard errors (optional)
+    double *grad_source;  // adjoint: 5 accumulators of sum_p grad_u[p] du_p/dtheta (zeroed)
+};
+
+cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &ps,
+                        uint64_t seed, const HeatDesc &h, int n_walks, double epsilon,
+                        int max_steps, double shell_delta, int precision, const FastPlan &plan,
+                        const uint8_t *location, const StartRecord *start, HeatPartial *partials,
+                        unsigned long long *queue, HeatOut out, DeviceCounters *counters,
+                        cudaStream_t stream, cudaEvent_t after_walk = nullptr);
+
 // Kernel-level checks.
 cudaError_t launch_prng(const uint64_t *seeds, long long n, int count, uint64_t *out,
                         cudaStream_t stream);

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kExactThreads)
         st.ny = q.y;
         st.nz = DIM == 3 ? q.z : 0.0;
         st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
-        st.pad = 0;
+        st.slot = q.slot;
         int where;
         if (DIM == 2) {
             where = st.radius <= btol ? 2 : (winding_number(s, p[0], p[1]) != 0 ? 1 : 0);

@@ -21,25 +21,12 @@
 #include <cmath>
 #include <type_traits>
 
+#include "device/fast_walk.cuh"
 #include "kernels.h"
 
 namespace wosb {
 
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-template <typename T>
-struct FastRng {
-    PhiloxStream s;
-    __device__ FastRng(uint64_t pseed, uint32_t walk) : s(pseed, walk) {}
-    __device__ __forceinline__ T unit();
-    __device__ __forceinline__ T unit_open() { return unit(); }
-};
-template <>
-__device__ __forceinline__ float FastRng<float>::unit() { return s.uniform_f(); }
-template <>
-__device__ __forceinline__ double FastRng<double>::unit() { return s.uniform_d(); }
 
 struct FastArgs {
     SceneView s;
@@ -66,54 +53,6 @@ struct FastArgs {
     unsigned long long *queue;
     DeviceCounters *ctr;
 };
-
-__device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000LL); }
-
-// Chan et al. pairwise combination of (n, mean, M2).
-__device__ __forceinline__ void chan_merge(double &n, double &mean, double &m2, double nb,
-                                           double meanb, double m2b) {
-    if (nb == 0.0) return;
-    if (n == 0.0) {
-        n = nb;
-        mean = meanb;
-        m2 = m2b;
-        return;
-    }
-    const double tot = n + nb;
-    const double delta = meanb - mean;
-    mean += delta * (nb / tot);
-    m2 += m2b + delta * delta * (n * nb / tot);
-    n = tot;
-}
-
-template <int DIM>
-__device__ __forceinline__ int bid_of(const SceneView &s, int slot) {
-    return (DIM == 2 && slot >= 0) ? s.segid[slot].x : -1;
-}
-
-// FP64 re-projection of p onto the primitive in `slot` (the FP32 query's
-// winner): exact distance, nearest point and (2D) boundary id.
-template <int DIM>
-__device__ __forceinline__ double reproject64(const SceneView &s, int slot, double px, double py,
-                                              double pz, V3<double> &np, int &bid) {
-    // `slot` is a binary-tree slot (the FP64 records' order)
-    if (DIM == 2) {
-        const double2 a = s.seg64[2 * slot], c = s.seg64[2 * slot + 1];
-        double nx, ny;
-        const double d2 = npq_seg64(a.x, a.y, c.x, c.y, px, py, nx, ny);
-        np = V3<double>{nx, ny, 0.0};
-        bid = s.segid[slot].x;
-        return sqrt(d2);
-    }
-    const double2 *r = s.tri64 + 7 * slot;
-    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5], r6 = r[6];
-    double nx, ny, nz;
-    const double d2 = eberly<double>(px, py, pz, r0.x, r0.y, r1.x, r1.y, r2.x, r2.y, r3.x, r3.y,
-                                     r4.x, r4.y, r5.x, r5.y, r6.x, r6.y, nx, ny, nz);
-    np = V3<double>{nx, ny, nz};
-    bid = -1;
-    return sqrt(d2);
-}
 
 template <int DIM, class Eq, typename T, int MIN_BLOCKS>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, Eq eq) {

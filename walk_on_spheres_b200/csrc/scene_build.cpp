@@ -528,6 +528,10 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
             o[15] = static_cast<float>(1.0 / fc);
         }
     }
+    sc.slot_verts.resize(static_cast<size_t>(n_prims) * dim);
+    for (int s = 0; s < n_prims; ++s) {
+        for (int k = 0; k < dim; ++k) sc.slot_verts[dim * s + k] = prims[dim * sc.order[s] + k];
+    }
     build_wide(sc, B.items, dim);
     return std::string();
 }

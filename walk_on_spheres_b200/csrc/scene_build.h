@@ -32,6 +32,7 @@ struct HostScene {
     std::vector<float> wbox;     // dim*2 arrays of w_box_total: lo.x lo.y [lo.z] hi.x hi.y [hi.z]
     std::vector<float> wprim;    // 2D: x0 y0 vx vy inv; 3D: v0 e1 e2 a b c det 1/det 1/a 1/c (16)
     std::vector<int> wide2bin;   // wide slot -> binary-tree slot (FP64 records), -1 for padding
+    std::vector<int> slot_verts; // binary-tree slot -> the primitive's dim vertex ids
     // the mesh itself (for the adjoint's per-vertex data and the checks)
     std::vector<double> verts;
     std::vector<int> prims;
