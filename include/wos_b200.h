@@ -183,6 +183,57 @@ int wos_solve_points(wos_context *ctx, const wos_params *params, const double *p
                      double *standard_error, double *mean_steps, uint8_t *location,
                      wos_counters *counters);
 
+/* ----------------------------------------------------------------- batches */
+
+/* Many independent grid sweeps, each with its own mesh, grid, equation,
+ * walk count and seed, run together (no reference counterpart: the reference
+ * runs one registry entry per process).  Each solve means exactly what
+ * wos_solve_grid means for the same arguments and FAST method: under the
+ * same chunking (wos_set_tuning / wos_batch_set_tuning) every walk draws the
+ * same numbers and takes the same steps, so locations, step counts and
+ * counters are identical and the statistics differ at most by the rounding
+ * of the terminal FP64 arithmetic (the batch kernel is compiled apart from
+ * the single-solve kernel).  The batch runs one classification launch per
+ * dimension, one persistent walk launch per (dimension, equation, method)
+ * family over a device work queue of (solve, point, chunk-of-walks) tasks,
+ * and one merge launch; wos_batch_run can capture that sequence once as a
+ * CUDA graph and replay it. */
+typedef struct wos_batch wos_batch;
+
+/* A batch on the context's device and stream.  The context's own mesh and
+ * buffers are untouched. */
+int wos_batch_create(wos_context *ctx, wos_batch **out);
+void wos_batch_destroy(wos_batch *batch);
+
+/* Add a mesh (arguments as wos_set_mesh); *mesh_id indexes it. */
+int wos_batch_add_mesh(wos_batch *batch, int dim, const double *verts, int n_verts,
+                       const int *prims, int n_prims, const int *boundary_ids, int leaf_size,
+                       int *mesh_id);
+
+/* Add a sweep of `grid` over mesh `mesh_id` (params as wos_solve_grid; the
+ * method must be FAST_FP32 or FAST_FP64).  *solve_id indexes it. */
+int wos_batch_add_solve(wos_batch *batch, int mesh_id, const wos_params *params,
+                        const wos_grid *grid, int *solve_id);
+
+/* Walks per task (<= 0: min(N_walks, 1024) per solve) and persistent grid
+ * size of every walk launch (<= 0: every block that can be resident). */
+int wos_batch_set_tuning(wos_batch *batch, int chunk, int blocks);
+
+/* Run every solve.  use_graph != 0 captures the launch sequence as a CUDA
+ * graph on the first run (and after any change to the batch) and replays
+ * it.  *device_ms (may be NULL) is the device time of the whole batch. */
+int wos_batch_run(wos_batch *batch, int use_graph, float *device_ms);
+
+/* Totals of the batch: solves, grid points, walks of the last run. */
+int wos_batch_info(const wos_batch *batch, int *n_solves, long long *n_points,
+                   long long *total_walks, long long *total_steps);
+
+/* Fields (host arrays of the solve's Nx*Ny*Nz points, any may be NULL) and
+ * counters of solve `solve_id` from the last run. */
+int wos_batch_result(wos_batch *batch, int solve_id, double *mean, double *variance,
+                     double *standard_error, double *mean_steps, uint8_t *location,
+                     wos_counters *counters);
+
 /* ------------------------------------ Gaussian heat source and its adjoint */
 
 /* Source of the differentiable heat problem (no reference counterpart; the

@@ -88,6 +88,16 @@ SIGNATURES = {
     "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
     "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
+    "wos_batch_create": (C.c_int, [VP, C.POINTER(VP)]),
+    "wos_batch_destroy": (None, [VP]),
+    "wos_batch_add_mesh": (C.c_int, [VP, C.c_int, VP, C.c_int, VP, C.c_int, VP, C.c_int,
+                                     C.POINTER(C.c_int)]),
+    "wos_batch_add_solve": (C.c_int, [VP, C.c_int, C.POINTER(Params), C.POINTER(Grid),
+                                      C.POINTER(C.c_int)]),
+    "wos_batch_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_batch_run": (C.c_int, [VP, C.c_int, C.POINTER(C.c_float)]),
+    "wos_batch_info": (C.c_int, [VP, C.POINTER(C.c_int)] + [C.POINTER(C.c_longlong)] * 3),
+    "wos_batch_result": (C.c_int, [VP, C.c_int] + [VP] * 5 + [C.POINTER(Counters)]),
     "wos_heat_forward": (C.c_int, [VP, C.POINTER(Params), C.POINTER(GaussianSource), VP, VP, VP,
                                    C.c_longlong] + [VP] * 5 + [C.POINTER(Counters)]),
     "wos_heat_adjoint": (C.c_int, [VP, C.POINTER(Params), C.POINTER(GaussianSource), VP, VP, VP,

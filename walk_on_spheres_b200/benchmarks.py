@@ -1,6 +1,7 @@
 """Throughput and accuracy of the single-solve workloads, per walk method.
 
     python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks --batch [--scale 1.0]
 
 Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 
@@ -13,6 +14,9 @@ Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 * screened3d_sphere16128_64cube — `screened_poisson`, alpha 10, on the UV
   sphere with 128 x 64 bands (16 128 triangles), 64^3 grid, 1024 walks,
   seed 7 (eps clamped to 0.005).
+
+`--batch` runs the 64-solve mixed batch (mixed_batch_specs) as one
+graph-captured launch sequence and, for comparison, solve by solve.
 
 For each workload and method it prints device walks/s, closest-point
 queries/s, mean steps and, against PLAIN_FP64 (the reference estimator and
@@ -119,13 +123,103 @@ def run(name: str, scale: float = 1.0, device: int = 0) -> dict:
     return out
 
 
+EQUATIONS3 = ("laplace", "poisson", "screened_poisson")
+
+
+def mixed_batch_specs(seed: int = 2024, scale: float = 1.0) -> list[dict]:
+    """The mixed batch of 64 independent solves: 32 star polygons
+    r = 1 + 0.3 sum_{k<=6} a_k cos(k theta + phi_k) (a_k ~ U[0, 0.15]) with
+    64..4096 edges (log-uniform) on square grids of side 32..512, and 32 UV
+    spheres radially perturbed by real spherical harmonics up to degree 4 with
+    2k..200k triangles on cubic grids of side 16..64; N_walks from
+    {256, 1024, 4096}, equation from laplace / poisson / screened_poisson
+    (alpha ~ U[1, 20]), source mode uniform or Green, one seed per solve.
+    `scale` multiplies the walk counts."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k in range(64):
+        dim = 2 if k < 32 else 3
+        if dim == 2:
+            edges = int(round(np.exp(rng.uniform(np.log(64), np.log(4096)))))
+            side = int(round(np.exp(rng.uniform(np.log(32), np.log(512)))))
+            mesh = dict(kind="star", edges=edges, seed=int(rng.integers(1 << 31)))
+            grid = (side, side, 1)
+        else:
+            tris = np.exp(rng.uniform(np.log(2000), np.log(200000)))
+            lon = max(8, int(round(np.sqrt(tris))))
+            mesh = dict(kind="sphere", lon=lon, lat=max(4, lon // 2),
+                        seed=int(rng.integers(1 << 31)))
+            side = int(round(np.exp(rng.uniform(np.log(16), np.log(64)))))
+            grid = (side, side, side)
+        walks = int(rng.choice([256, 1024, 4096]))
+        eq = EQUATIONS3[int(rng.integers(3))]
+        alpha = float(rng.uniform(1.0, 20.0))
+        mode = ("uniform", "green")[int(rng.integers(2))]
+        specs.append(dict(dim=dim, mesh=mesh, grid=grid, equation=eq,
+                          params=dict(N_walks=max(1, int(round(walks * scale))), alpha=alpha,
+                                      source_mode=mode, seed=int(rng.integers(1 << 62)),
+                                      method="fast")))
+    return specs
+
+
+def build_mesh(m: dict):
+    rng = np.random.default_rng(m["seed"])
+    if m["kind"] == "star":
+        return meshes.star_polygon(rng, m["edges"])
+    return meshes.perturbed_sphere(rng, m["lon"], m["lat"])
+
+
+def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
+              seed: int = 2024) -> dict:
+    """Device time of the mixed batch as one graph-captured launch sequence,
+    against the same solves run one after another (sum of their device
+    times)."""
+    from .batch import Batch
+    specs = mixed_batch_specs(seed, scale)
+    s = Solver(device)
+    b = Batch(s)
+    built = []
+    for sp in specs:
+        mesh = build_mesh(sp["mesh"])
+        built.append(mesh)
+        mid = b.add_mesh(mesh)
+        b.add_solve(mid, sp["equation"], *sp["grid"], **sp["params"])
+    b.run(use_graph=True)            # plan, capture, warm
+    ms = b.run(use_graph=True)
+    info = b.info()
+    out = {"workload": "mixed_batch_64", "scale": scale, "solves": info["solves"],
+           "points": info["points"], "walks": info["walks"], "steps": info["steps"],
+           "prims": [int(m.prims.shape[0]) for m in built],
+           "batch_graph_ms": ms, "batch_walks_per_s": info["walks"] / (ms / 1000.0),
+           "batch_queries_per_s": info["steps"] / (ms / 1000.0)}
+    ms_stream = b.run(use_graph=False)
+    out["batch_stream_ms"] = ms_stream
+    b.close()
+    if sequential:
+        total = 0.0
+        for sp, mesh in zip(specs, built):
+            s.set_mesh(mesh)
+            r = s.solve_grid(sp["equation"], *sp["grid"], **sp["params"])
+            total += r.counters["total_ms"]
+        out["sequential_ms"] = total
+        out["sequential_walks_per_s"] = info["walks"] / (total / 1000.0)
+        out["batch_speedup"] = total / ms
+    s.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--workloads", default=",".join(WORKLOADS))
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--batch", action="store_true",
+                    help="run the 64-solve mixed batch instead of the single solves")
     a = ap.parse_args(argv)
+    if a.batch:
+        print(json.dumps(run_batch(a.scale, a.device)), flush=True)
+        return 0
     for name in a.workloads.split(","):
         print(json.dumps(run(name.strip(), a.scale, a.device)), flush=True)
     return 0

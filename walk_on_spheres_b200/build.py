@@ -43,6 +43,7 @@ CUDA_UNITS = {
     # host code that includes the device headers' type definitions
     "context.cpp": ["-x", "cu"],
     "heat_api.cpp": ["-x", "cu"],
+    "batch.cpp": ["-x", "cu"],
     "noalloc.cu": [],
 }
 HOST_UNITS = ["scene_build.cpp", "obj_reader.cpp", "runner.cpp", "h5_writer.cpp", "host_api.cpp"]

@@ -63,6 +63,7 @@ static cudaError_t upload(DeviceBuffer &b, const std::vector<T> &v, cudaStream_t
 
 wos_context::~wos_context() {
     for (DeviceBuffer *b : all_buffers()) b->release();
+    sdev.release();
     for (auto &ev : events) {
         if (ev) cudaEventDestroy(ev);
     }
@@ -70,7 +71,7 @@ wos_context::~wos_context() {
 }
 
 std::vector<DeviceBuffer *> wos_context::all_buffers() {
-    return {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32, &wbox, &wprim, &wide2bin, &woff, &slotv, &location, &start,
+    return {&location, &start,
             &f_mean, &f_var, &f_se, &f_steps, &f_loc, &partials, &queue, &counters, &points,
             &index, &scratch_a, &scratch_b, &scratch_c, &scratch_d, &h_values, &h_gradu,
             &h_gradg, &h_grads, &h_jac, &h_jacse};
@@ -129,29 +130,32 @@ extern "C" void wos_context_destroy(wos_context *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (wos_batch *b : ctx->batches) detach_batch(b);
+    ctx->batches.clear();
     delete ctx;
 }
 
 // ------------------------------------------------------------- mesh
 
-int wos_context::upload_scene() {
-    cudaSetDevice(device);
-    const HostScene &h = scene;
-    WOS_CUDA(this, upload(box64, h.box64, stream), "upload BVH boxes");
-    WOS_CUDA(this, upload(seg64, h.seg64, stream), "upload segments");
-    WOS_CUDA(this, upload(segid, h.segid, stream), "upload segment ids");
-    WOS_CUDA(this, upload(tri64, h.tri64, stream), "upload triangles");
-    WOS_CUDA(this, upload(pair32, h.pair32, stream), "upload FP32 boxes");
-    WOS_CUDA(this, upload(seg32, h.seg32, stream), "upload FP32 segments");
-    WOS_CUDA(this, upload(seg32inv, h.seg32inv, stream), "upload FP32 segment reciprocals");
-    WOS_CUDA(this, upload(tri32, h.tri32, stream), "upload FP32 triangles");
-    WOS_CUDA(this, upload(wbox, h.wbox, stream), "upload wide boxes");
-    WOS_CUDA(this, upload(wprim, h.wprim, stream), "upload wide primitives");
-    WOS_CUDA(this, upload(wide2bin, h.wide2bin, stream), "upload wide slot map");
-    WOS_CUDA(this, upload(slotv, h.slot_verts, stream), "upload slot vertex ids");
-    WOS_CUDA(this, upload(woff, std::vector<int>(h.w_off, h.w_off + 8), stream),
-             "upload wide offsets");
-    WOS_CUDA(this, cudaStreamSynchronize(stream), "mesh upload");
+cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
+    cudaError_t e;
+#define WOS_UP(buf, vec) \
+    if ((e = ::upload(buf, vec, stream)) != cudaSuccess) return e
+    WOS_UP(box64, h.box64);
+    WOS_UP(seg64, h.seg64);
+    WOS_UP(segid, h.segid);
+    WOS_UP(tri64, h.tri64);
+    WOS_UP(pair32, h.pair32);
+    WOS_UP(seg32, h.seg32);
+    WOS_UP(seg32inv, h.seg32inv);
+    WOS_UP(tri32, h.tri32);
+    WOS_UP(wbox, h.wbox);
+    WOS_UP(wprim, h.wprim);
+    WOS_UP(wide2bin, h.wide2bin);
+    WOS_UP(woff, std::vector<int>(h.w_off, h.w_off + 8));
+    WOS_UP(slotv, h.slot_verts);
+#undef WOS_UP
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     view = SceneView{};
     view.dim = h.dim;
     view.n_prims = h.n_prims;
@@ -174,6 +178,21 @@ int wos_context::upload_scene() {
     wide.box = static_cast<const float *>(wbox.ptr);
     wide.prim = static_cast<const float *>(wprim.ptr);
     wide.wide2bin = static_cast<const int *>(wide2bin.ptr);
+    return cudaSuccess;
+}
+
+void SceneDevice::release() {
+    for (DeviceBuffer *b : {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32,
+                            &wbox, &wprim, &wide2bin, &woff, &slotv}) {
+        b->release();
+    }
+}
+
+int wos_context::upload_scene() {
+    cudaSetDevice(device);
+    WOS_CUDA(this, sdev.upload(scene, stream), "mesh upload");
+    view = sdev.view;
+    wide = sdev.wide;
     has_mesh = true;
     return WOS_OK;
 }

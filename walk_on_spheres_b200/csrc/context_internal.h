@@ -19,7 +19,23 @@ struct DeviceBuffer {
     void release();
 };
 
+// Device copy of one HostScene (all tree and primitive arrays) and the
+// views the kernels take.
+struct SceneDevice {
+    DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
+        wide2bin, woff, slotv;
+    SceneView view{};
+    WideView wide{};
+    // Uploads `h` on `stream` (synchronised) and fills view / wide.
+    cudaError_t upload(const HostScene &h, cudaStream_t stream);
+    void release();
+};
+
 double effective_epsilon(const wos_params &p);
+
+// Frees a batch's device memory and detaches it from its context (called
+// for every live batch when the context is destroyed).
+void detach_batch(wos_batch *batch);
 
 // Records `msg` as the context's (and the thread's) last error; returns code.
 int fail(wos_context *ctx, int code, const std::string &msg);
@@ -48,8 +64,7 @@ struct wos_context {
     wosb::WideView wide{};
 
     // scene
-    wosb::DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
-        wide2bin, woff, slotv;
+    wosb::SceneDevice sdev;
     // per solve
     wosb::DeviceBuffer location, start, f_mean, f_var, f_se, f_steps, f_loc, partials, queue,
         counters, points, index;
@@ -57,6 +72,9 @@ struct wos_context {
     wosb::DeviceBuffer scratch_a, scratch_b, scratch_c, scratch_d;
     // Gaussian heat source: vertex values, probe weights, gradients, Jacobian
     wosb::DeviceBuffer h_values, h_gradu, h_gradg, h_grads, h_jac, h_jacse;
+
+    // live batches created on this context (detached when it is destroyed)
+    std::vector<wos_batch *> batches;
 
     // tuning overrides (<= 0: automatic)
     int chunk_override = 0;

@@ -136,7 +136,7 @@ int prepare_heat(wos_context *ctx, const wos_params *params, const wos_gaussian_
     h.x0[1] = src->x0[1];
     h.x0[2] = src->x0[2];
     h.sigma = src->sigma;
-    h.slot_verts = static_cast<const int *>(ctx->slotv.ptr);
+    h.slot_verts = static_cast<const int *>(ctx->sdev.slotv.ptr);
     if (vertex_values) {
         const size_t nv = static_cast<size_t>(ctx->scene.n_verts);
         WOS_CUDA(ctx, ctx->h_values.reserve(sizeof(double) * nv), "alloc vertex values");

@@ -47,6 +47,71 @@ struct TaskPartial {
     unsigned int pad;
 };
 
+// Arguments of the fast walk kernel for one solve.
+struct FastArgs {
+    SceneView s;
+    WideView w;
+    PointSet ps;
+    uint64_t seed;
+    int n_walks;
+    double eps;
+    int max_steps;
+    double shell_delta;
+    float keep;     // (1 - tau)^2: approximate pruning bound of the FP32 query
+    float shrink;   // 1 - tau: conservative radius factor
+    float exact2;   // below this squared distance the FP32 query prunes exactly
+    float shell2;   // (eps + shell_delta)^2: FP32 radius inside the epsilon shell
+    int chunk;
+    int chunks;
+    long long n_tasks;
+    int stage;
+    int stage_box;   // floats of the wide box arrays staged in shared memory
+    int stage_prim;  // floats of the wide primitive arrays staged (0: read from global)
+    const uint8_t *location;
+    const StartRecord *start;
+    TaskPartial *partials;
+    unsigned long long *queue;
+    DeviceCounters *ctr;
+};
+
+// Fills the walk arguments of one solve (pruning bounds from epsilon and the
+// shell margin); the scene is never staged.
+FastArgs make_fast_args(const SceneView &s, const WideView &w, const PointSet &ps, uint64_t seed,
+                        int n_walks, double epsilon, int max_steps, double shell_delta,
+                        const FastPlan &plan, const uint8_t *location, const StartRecord *start,
+                        TaskPartial *partials, unsigned long long *queue, DeviceCounters *ctr);
+
+// One solve of a batch (many solves of different meshes, grids, equations
+// and walk counts run by one launch per walk family).  Point arrays are the
+// solve's own slices of the batch buffers.
+struct BatchItem {
+    FastArgs a;              // walk arguments (a.queue unused: one queue per family)
+    EqDesc eq;
+    Fields out;
+    double btol;             // boundary tolerance of the classification
+    int max_ray_attempts;
+    int precision;           // 32 / 64
+    long long point_begin;   // first point of the solve in the batch's point order
+    long long task_begin;    // first task of the solve in its family's queue
+};
+
+// Classification of the points [point_base, point_base + n_points) of the
+// batch items [0, n_items) (all of one dimension, sorted by point_begin).
+cudaError_t launch_classify_batch(int dim, const BatchItem *items, int n_items,
+                                  long long point_base, long long n_points, cudaStream_t stream);
+
+// Fast walks of one family (all items share dim, equation kind and
+// precision; tasks numbered by task_begin from 0) on a persistent grid of
+// `blocks` blocks (batch_walk_blocks: every block that can be resident).
+cudaError_t launch_walk_batch(int dim, int kind, int precision, const BatchItem *items,
+                              int n_items, long long n_tasks, unsigned long long *queue,
+                              int blocks, cudaStream_t stream);
+cudaError_t batch_walk_blocks(int dim, int kind, int precision, int *blocks);
+
+// Per-point merge of every item of the batch.
+cudaError_t launch_merge_batch(const BatchItem *items, int n_items, long long n_points,
+                               cudaStream_t stream);
+
 // FAST_FP32 (precision 32) / FAST_FP64 (precision 64) walks over all tasks,
 // then the per-point merge into the output fields.
 cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointSet &ps,

@@ -43,6 +43,51 @@ __device__ int classify_3d(const SceneView &s, const double *p, double bdist, do
     return votes > 1 ? 1 : 0;
 }
 
+// Start point, location and (non-inside) fields of point t of `ps`
+// (include/wos/runner.hpp:170-206).
+template <int DIM>
+__device__ __forceinline__ void classify_point(const SceneView &s, const PointSet &ps,
+                                               long long t, uint64_t seed, int max_ray_attempts,
+                                               double btol, const EqDesc &eq, const Fields &out,
+                                               uint8_t *location, StartRecord *start,
+                                               DeviceCounters *ctr) {
+    double p[3];
+    uint64_t linear;
+    point_at(ps, t, p[0], p[1], p[2], linear);
+    const Nearest<double> q = nearest64<DIM>(s, p[0], p[1], p[2], dinf());
+    StartRecord st;
+    st.radius = sqrt(q.best);
+    st.nx = q.x;
+    st.ny = q.y;
+    st.nz = DIM == 3 ? q.z : 0.0;
+    st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
+    st.slot = q.slot;
+    int where;
+    if (DIM == 2) {
+        where = st.radius <= btol ? 2 : (winding_number(s, p[0], p[1]) != 0 ? 1 : 0);
+    } else {
+        Xoshiro rng(splitmix64(point_seed(seed, linear) ^ kInsideStream));
+        int retries = 0;
+        where = classify_3d(s, p, st.radius, btol, max_ray_attempts, rng, retries);
+        if (retries) atomicAdd(&ctr->ambiguous_ray_retries, static_cast<unsigned long long>(retries));
+        if (where == 3) atomicAdd(&ctr->indeterminate_points, 1ull);
+    }
+    location[t] = static_cast<uint8_t>(where);
+    start[t] = st;
+    if (out.location) out.location[t] = static_cast<uint8_t>(where);
+    if (where != 1) {
+        double m = __longlong_as_double(0x7ff8000000000000LL), zero = m;
+        if (where == 2) {
+            m = boundary_value<DIM>(eq, V3<double>{st.nx, st.ny, st.nz}, st.boundary_id);
+            zero = 0.0;
+        }
+        if (out.mean) out.mean[t] = m;
+        if (out.variance) out.variance[t] = zero;
+        if (out.standard_error) out.standard_error[t] = zero;
+        if (out.mean_steps) out.mean_steps[t] = zero;
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kExactThreads)
     classify_kernel(SceneView s, PointSet ps, uint64_t seed, int max_ray_attempts, double btol,
@@ -51,41 +96,30 @@ __global__ void __launch_bounds__(kExactThreads)
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < ps.n;
          t += stride) {
-        double p[3];
-        uint64_t linear;
-        point_at(ps, t, p[0], p[1], p[2], linear);
-        const Nearest<double> q = nearest64<DIM>(s, p[0], p[1], p[2], dinf());
-        StartRecord st;
-        st.radius = sqrt(q.best);
-        st.nx = q.x;
-        st.ny = q.y;
-        st.nz = DIM == 3 ? q.z : 0.0;
-        st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
-        st.slot = q.slot;
-        int where;
-        if (DIM == 2) {
-            where = st.radius <= btol ? 2 : (winding_number(s, p[0], p[1]) != 0 ? 1 : 0);
-        } else {
-            Xoshiro rng(splitmix64(point_seed(seed, linear) ^ kInsideStream));
-            int retries = 0;
-            where = classify_3d(s, p, st.radius, btol, max_ray_attempts, rng, retries);
-            if (retries) atomicAdd(&ctr->ambiguous_ray_retries, static_cast<unsigned long long>(retries));
-            if (where == 3) atomicAdd(&ctr->indeterminate_points, 1ull);
+        classify_point<DIM>(s, ps, t, seed, max_ray_attempts, btol, eq, out, location, start, ctr);
+    }
+}
+
+// Classification of a batch: global point g in [base, base + n) belongs to
+// the item with the largest point_begin <= g.
+template <int DIM>
+__global__ void __launch_bounds__(kExactThreads)
+    classify_batch_kernel(const BatchItem *__restrict__ items, int n_items, long long base,
+                          long long n) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
+         t += stride) {
+        const long long g = base + t;
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].point_begin <= g) lo = mid;
+            else hi = mid - 1;
         }
-        location[t] = static_cast<uint8_t>(where);
-        start[t] = st;
-        if (out.location) out.location[t] = static_cast<uint8_t>(where);
-        if (where != 1) {
-            double m = __longlong_as_double(0x7ff8000000000000LL), zero = m;
-            if (where == 2) {
-                m = boundary_value<DIM>(eq, V3<double>{st.nx, st.ny, st.nz}, st.boundary_id);
-                zero = 0.0;
-            }
-            if (out.mean) out.mean[t] = m;
-            if (out.variance) out.variance[t] = zero;
-            if (out.standard_error) out.standard_error[t] = zero;
-            if (out.mean_steps) out.mean_steps[t] = zero;
-        }
+        const BatchItem &it = items[lo];
+        classify_point<DIM>(it.a.s, it.a.ps, g - it.point_begin, it.a.seed, it.max_ray_attempts,
+                            it.btol, it.eq, it.out, const_cast<uint8_t *>(it.a.location),
+                            const_cast<StartRecord *>(it.a.start), it.a.ctr);
     }
 }
 
@@ -237,6 +271,21 @@ cudaError_t launch_classify(const SceneView &s, const PointSet &ps, uint64_t see
         classify_kernel<3><<<blocks, kExactThreads, 0, stream>>>(s, ps, seed, max_ray_attempts,
                                                                  btol, eq, out, location, start,
                                                                  counters);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_classify_batch(int dim, const BatchItem *items, int n_items,
+                                  long long point_base, long long n_points, cudaStream_t stream) {
+    if (n_items <= 0 || n_points <= 0) return cudaSuccess;
+    long long b = (n_points + kExactThreads - 1) / kExactThreads;
+    if (b > 148 * 64) b = 148 * 64;
+    if (dim == 2) {
+        classify_batch_kernel<2><<<static_cast<int>(b), kExactThreads, 0, stream>>>(
+            items, n_items, point_base, n_points);
+    } else {
+        classify_batch_kernel<3><<<static_cast<int>(b), kExactThreads, 0, stream>>>(
+            items, n_items, point_base, n_points);
     }
     return cudaGetLastError();
 }

@@ -28,31 +28,204 @@ namespace wosb {
 
 namespace {
 
-struct FastArgs {
-    SceneView s;
-    WideView w;
-    PointSet ps;
-    uint64_t seed;
-    int n_walks;
-    double eps;
-    int max_steps;
-    double shell_delta;
-    float keep;     // (1 - tau)^2: approximate pruning bound of the FP32 query
-    float shrink;   // 1 - tau: conservative radius factor
-    float exact2;   // below this squared distance the FP32 query prunes exactly
-    float shell2;   // (eps + shell_delta)^2: FP32 radius inside the epsilon shell
-    int chunk;
-    int chunks;
-    long long n_tasks;
-    int stage;
-    int stage_box;   // floats of the wide box arrays staged in shared memory
-    int stage_prim;  // floats of the wide primitive arrays staged (0: read from global)
-    const uint8_t *location;
-    const StartRecord *start;
-    TaskPartial *partials;
-    unsigned long long *queue;
-    DeviceCounters *ctr;
-};
+
+// One task: walks [c*chunk, min(N, (c+1)*chunk)) of point pidx, written to
+// a.partials[task] as Welford statistics.
+template <int DIM, class Eq, typename T>
+__device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, const Eq &eq,
+                                          unsigned long long task, long long pidx, int c) {
+    constexpr bool kF32 = std::is_same<T, float>::value;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const double eps = a.eps;
+
+    double x0, y0, z0;
+    uint64_t linear;
+    point_at(a.ps, pidx, x0, y0, z0, linear);
+    const uint64_t pseed = point_seed(a.seed, linear);
+    const V3<T> p0{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
+    const double r0 = a.start[pidx].radius;
+    const T R0 = static_cast<T>(r0);
+    const bool start_stops = !(r0 > eps);  // start point already inside the shell
+    const int w0 = c * a.chunk;
+    const int w1 = min(a.n_walks, w0 + a.chunk);
+
+    // per-lane statistics
+    int n_acc = 0, steps_acc = 0;
+    double mean_acc = 0.0, m2_acc = 0.0;
+    unsigned hits = 0;
+    bool overflow = false;
+
+    // per-lane walk state
+    int walk = w0 + lane;
+    bool active = walk < w1;
+    int next = w0 + 32;
+    V3<T> p = p0;
+    T R = R0;
+    T sample = T(0), weight = T(1);
+    int steps = 0;
+    int slot = -1;                 // FP32: winner of the last query
+    V3<double> np64{0.0, 0.0, 0.0};  // FP64: nearest point of the last query
+    int bid64 = -1;
+    FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
+
+    while (__any_sync(kFull, active)) {
+        bool done = false;
+        bool need_query = false;
+        double value = 0.0;
+        if (active) {
+            bool stop = false;
+            V3<double> np{0.0, 0.0, 0.0};
+            int bid = -1;
+            if (steps == 0) {
+                stop = start_stops;
+                if (stop) {
+                    const StartRecord st = a.start[pidx];
+                    np = V3<double>{st.nx, st.ny, st.nz};
+                    bid = st.boundary_id;
+                }
+            } else if (!kF32) {
+                stop = !(static_cast<double>(R) > eps);
+                np = np64;
+                bid = bid64;
+            } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
+                // epsilon shell: FP64 re-projection onto the nearest primitive
+                const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
+                                                    static_cast<double>(p.x),
+                                                    static_cast<double>(p.y),
+                                                    static_cast<double>(p.z), np, bid);
+                if (d64 <= eps) {
+                    stop = true;
+                } else {
+                    R = static_cast<T>(d64);
+                }
+            }
+            if (!stop && steps >= a.max_steps) {
+                // step cap: finish at the nearest boundary point
+                // (include/wos/wos.hpp:129-137)
+                ++hits;
+                stop = true;
+                if (kF32) {
+                    reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
+                                     static_cast<double>(p.y), static_cast<double>(p.z), np,
+                                     bid);
+                } else {
+                    np = np64;
+                    bid = bid64;
+                }
+            }
+            if (stop) {
+                value = static_cast<double>(sample) +
+                        static_cast<double>(weight) * eq.boundary(np, bid);
+                done = true;
+            } else {
+                p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
+                ++steps;
+                if constexpr (kF32) {
+                    need_query = true;
+                } else {
+                    const Nearest<double> q = nearest64<DIM>(
+                        a.s, static_cast<double>(p.x), static_cast<double>(p.y),
+                        static_cast<double>(p.z), dinf());
+                    R = static_cast<T>(sqrt(q.best));
+                    np64 = V3<double>{q.x, q.y, q.z};
+                    bid64 = bid_of<DIM>(a.s, q.slot);
+                }
+            }
+        }
+        if constexpr (kF32) {
+            // the warp resolves every pending closest-point query together
+            unsigned pending = __ballot_sync(kFull, need_query);
+            float qbest = 0.0f;
+            int qslot = -1;
+            while (pending) {
+                const int j = __ffs(pending) - 1;
+                pending &= pending - 1u;
+                const float qx = __shfl_sync(kFull, static_cast<float>(p.x), j);
+                const float qy = __shfl_sync(kFull, static_cast<float>(p.y), j);
+                const float qz = DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), j) : 0.0f;
+                const WideResult r = wide_nearest<DIM>(wv, qx, qy, qz, a.keep, a.exact2);
+                if (lane == j) {
+                    qbest = r.best;
+                    qslot = r.slot;
+                }
+            }
+            if (need_query) {
+                const float r = sqrtf(qbest);
+                R = static_cast<T>(qbest > a.shell2 ? r * a.shrink : r);
+                slot = qslot;
+            }
+        }
+        if (done) {
+            // Welford update of this lane's statistics
+            ++n_acc;
+            const double before = value - mean_acc;
+            mean_acc += before / static_cast<double>(n_acc);
+            m2_acc += before * (value - mean_acc);
+            steps_acc += steps;
+        }
+        const unsigned done_mask = __ballot_sync(kFull, done);
+        if (done_mask) {
+            if (done) {
+                walk = next + __popc(done_mask & lt_mask);
+                active = walk < w1;
+                if (active) {
+                    p = p0;
+                    R = R0;
+                    sample = T(0);
+                    weight = T(1);
+                    steps = 0;
+                    rng = FastRng<T>(pseed, static_cast<uint32_t>(walk));
+                }
+            }
+            next += __popc(done_mask);
+        }
+    }
+
+    // warp merge of the lanes' statistics
+    double n_tot = static_cast<double>(n_acc);
+    unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double nb = __shfl_down_sync(kFull, n_tot, o);
+        const double mb = __shfl_down_sync(kFull, mean_acc, o);
+        const double m2b = __shfl_down_sync(kFull, m2_acc, o);
+        const unsigned long long sb = __shfl_down_sync(kFull, steps_tot, o);
+        const unsigned hb = __shfl_down_sync(kFull, hits, o);
+        chan_merge(n_tot, mean_acc, m2_acc, nb, mb, m2b);
+        steps_tot += sb;
+        hits += hb;
+    }
+    const unsigned any_overflow = __ballot_sync(kFull, overflow);
+    if (lane == 0) {
+        TaskPartial tp;
+        tp.n = n_tot;
+        tp.mean = mean_acc;
+        tp.m2 = m2_acc;
+        tp.steps = static_cast<double>(steps_tot);
+        tp.hits = hits;
+        tp.pad = 0;
+        a.partials[task] = tp;
+        if (any_overflow) atomicOr(&a.ctr->error_flags, kErrRejectionCap);
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ Laplace<DIM> eq_from(const EqDesc &, Laplace<DIM> *) {
+    return Laplace<DIM>{};
+}
+template <int DIM>
+__device__ __forceinline__ Poisson<DIM> eq_from(const EqDesc &e, Poisson<DIM> *) {
+    return Poisson<DIM>{e.mode, e.alpha};
+}
+template <int DIM>
+__device__ __forceinline__ Screened<DIM> eq_from(const EqDesc &e, Screened<DIM> *) {
+    return Screened<DIM>{e.mode, e.alpha};
+}
+template <int DIM>
+__device__ __forceinline__ Helmholtz<DIM> eq_from(const EqDesc &, Helmholtz<DIM> *) {
+    return Helmholtz<DIM>{};
+}
 
 template <int DIM, class Eq, typename T, int MIN_BLOCKS>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, Eq eq) {
@@ -74,8 +247,6 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, 
         if (a.stage_prim) wv.prim = sm + a.stage_box;
     }
     const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const double eps = a.eps;
 
     for (;;) {
         unsigned long long task = 0;
@@ -85,180 +256,74 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, 
         const long long pidx = static_cast<long long>(task / a.chunks);
         const int c = static_cast<int>(task % a.chunks);
         if (a.location[pidx] != 1) continue;
+        fast_task<DIM, Eq, T>(a, wv, eq, task, pidx, c);
+    }
+}
 
-        double x0, y0, z0;
-        uint64_t linear;
-        point_at(a.ps, pidx, x0, y0, z0, linear);
-        const uint64_t pseed = point_seed(a.seed, linear);
-        const V3<T> p0{static_cast<T>(x0), static_cast<T>(y0), static_cast<T>(z0)};
-        const double r0 = a.start[pidx].radius;
-        const T R0 = static_cast<T>(r0);
-        const bool start_stops = !(r0 > eps);  // start point already inside the shell
-        const int w0 = c * a.chunk;
-        const int w1 = min(a.n_walks, w0 + a.chunk);
-
-        // per-lane statistics
-        int n_acc = 0, steps_acc = 0;
-        double mean_acc = 0.0, m2_acc = 0.0;
-        unsigned hits = 0;
-        bool overflow = false;
-
-        // per-lane walk state
-        int walk = w0 + lane;
-        bool active = walk < w1;
-        int next = w0 + 32;
-        V3<T> p = p0;
-        T R = R0;
-        T sample = T(0), weight = T(1);
-        int steps = 0;
-        int slot = -1;                 // FP32: winner of the last query
-        V3<double> np64{0.0, 0.0, 0.0};  // FP64: nearest point of the last query
-        int bid64 = -1;
-        FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
-
-        while (__any_sync(kFull, active)) {
-            bool done = false;
-            bool need_query = false;
-            double value = 0.0;
-            if (active) {
-                bool stop = false;
-                V3<double> np{0.0, 0.0, 0.0};
-                int bid = -1;
-                if (steps == 0) {
-                    stop = start_stops;
-                    if (stop) {
-                        const StartRecord st = a.start[pidx];
-                        np = V3<double>{st.nx, st.ny, st.nz};
-                        bid = st.boundary_id;
-                    }
-                } else if (!kF32) {
-                    stop = !(static_cast<double>(R) > eps);
-                    np = np64;
-                    bid = bid64;
-                } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
-                    // epsilon shell: FP64 re-projection onto the nearest primitive
-                    const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
-                                                        static_cast<double>(p.x),
-                                                        static_cast<double>(p.y),
-                                                        static_cast<double>(p.z), np, bid);
-                    if (d64 <= eps) {
-                        stop = true;
-                    } else {
-                        R = static_cast<T>(d64);
-                    }
-                }
-                if (!stop && steps >= a.max_steps) {
-                    // step cap: finish at the nearest boundary point
-                    // (include/wos/wos.hpp:129-137)
-                    ++hits;
-                    stop = true;
-                    if (kF32) {
-                        reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
-                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
-                                         bid);
-                    } else {
-                        np = np64;
-                        bid = bid64;
-                    }
-                }
-                if (stop) {
-                    value = static_cast<double>(sample) +
-                            static_cast<double>(weight) * eq.boundary(np, bid);
-                    done = true;
-                } else {
-                    p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
-                    ++steps;
-                    if constexpr (kF32) {
-                        need_query = true;
-                    } else {
-                        const Nearest<double> q = nearest64<DIM>(
-                            a.s, static_cast<double>(p.x), static_cast<double>(p.y),
-                            static_cast<double>(p.z), dinf());
-                        R = static_cast<T>(sqrt(q.best));
-                        np64 = V3<double>{q.x, q.y, q.z};
-                        bid64 = bid_of<DIM>(a.s, q.slot);
-                    }
-                }
-            }
-            if constexpr (kF32) {
-                // the warp resolves every pending closest-point query together
-                unsigned pending = __ballot_sync(kFull, need_query);
-                float qbest = 0.0f;
-                int qslot = -1;
-                while (pending) {
-                    const int j = __ffs(pending) - 1;
-                    pending &= pending - 1u;
-                    const float qx = __shfl_sync(kFull, static_cast<float>(p.x), j);
-                    const float qy = __shfl_sync(kFull, static_cast<float>(p.y), j);
-                    const float qz = DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), j) : 0.0f;
-                    const WideResult r = wide_nearest<DIM>(wv, qx, qy, qz, a.keep, a.exact2);
-                    if (lane == j) {
-                        qbest = r.best;
-                        qslot = r.slot;
-                    }
-                }
-                if (need_query) {
-                    const float r = sqrtf(qbest);
-                    R = static_cast<T>(qbest > a.shell2 ? r * a.shrink : r);
-                    slot = qslot;
-                }
-            }
-            if (done) {
-                // Welford update of this lane's statistics
-                ++n_acc;
-                const double before = value - mean_acc;
-                mean_acc += before / static_cast<double>(n_acc);
-                m2_acc += before * (value - mean_acc);
-                steps_acc += steps;
-            }
-            const unsigned done_mask = __ballot_sync(kFull, done);
-            if (done_mask) {
-                if (done) {
-                    walk = next + __popc(done_mask & lt_mask);
-                    active = walk < w1;
-                    if (active) {
-                        p = p0;
-                        R = R0;
-                        sample = T(0);
-                        weight = T(1);
-                        steps = 0;
-                        rng = FastRng<T>(pseed, static_cast<uint32_t>(walk));
-                    }
-                }
-                next += __popc(done_mask);
-            }
+// Walks of one family of batch items: one queue over the items' tasks
+// (numbered by task_begin); each task runs the walk_fast_kernel task body
+// with its own item's scene, grid, equation and statistics buffers (the
+// scene is read through L1/L2, never staged).
+template <int DIM, class Eq, typename T, int MIN_BLOCKS>
+__global__ void __launch_bounds__(256, MIN_BLOCKS)
+    walk_batch_kernel(const BatchItem *__restrict__ items, int n_items, long long n_tasks,
+                      unsigned long long *queue) {
+    __shared__ int s_off[8][8];  // per warp: wide-tree offsets of the warp's current item
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    int cur = -1;
+    for (;;) {
+        unsigned long long task = 0;
+        if (lane == 0) task = atomicAdd(queue, 1ull);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= static_cast<unsigned long long>(n_tasks)) break;
+        const long long t = static_cast<long long>(task);
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].task_begin <= t) lo = mid;
+            else hi = mid - 1;
         }
-
-        // warp merge of the lanes' statistics
-        double n_tot = static_cast<double>(n_acc);
-        unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double nb = __shfl_down_sync(kFull, n_tot, o);
-            const double mb = __shfl_down_sync(kFull, mean_acc, o);
-            const double m2b = __shfl_down_sync(kFull, m2_acc, o);
-            const unsigned long long sb = __shfl_down_sync(kFull, steps_tot, o);
-            const unsigned hb = __shfl_down_sync(kFull, hits, o);
-            chan_merge(n_tot, mean_acc, m2_acc, nb, mb, m2b);
-            steps_tot += sb;
-            hits += hb;
+        const BatchItem &it = items[lo];
+        if (lo != cur) {
+            __syncwarp();
+            if (lane < 8) s_off[warp][lane] = it.a.w.off[lane];
+            __syncwarp();
+            cur = lo;
         }
-        const unsigned any_overflow = __ballot_sync(kFull, overflow);
-        if (lane == 0) {
-            TaskPartial tp;
-            tp.n = n_tot;
-            tp.mean = mean_acc;
-            tp.m2 = m2_acc;
-            tp.steps = static_cast<double>(steps_tot);
-            tp.hits = hits;
-            tp.pad = 0;
-            a.partials[task] = tp;
-            if (any_overflow) atomicOr(&a.ctr->error_flags, kErrRejectionCap);
-        }
+        const long long local = t - it.task_begin;
+        const long long pidx = local / it.a.chunks;
+        const int c = static_cast<int>(local % it.a.chunks);
+        if (it.a.location[pidx] != 1) continue;
+        WideView wv = it.a.w;
+        wv.off = s_off[warp];
+        const Eq eq = eq_from(it.eq, static_cast<Eq *>(nullptr));
+        fast_task<DIM, Eq, T>(it.a, wv, eq, static_cast<unsigned long long>(local), pidx, c);
     }
 }
 
 // Per-point merge of the chunk statistics (include/wos/wos.hpp:182-190).
+__device__ __forceinline__ void merge_point(long long p, int chunks, int n_walks,
+                                            const TaskPartial *__restrict__ partials,
+                                            const Fields &out, DeviceCounters *ctr) {
+    double n = 0.0, mean = 0.0, m2 = 0.0, steps = 0.0;
+    unsigned long long hits = 0;
+    for (int c = 0; c < chunks; ++c) {
+        const TaskPartial tp = partials[p * chunks + c];
+        chan_merge(n, mean, m2, tp.n, tp.mean, tp.m2);
+        steps += tp.steps;
+        hits += tp.hits;
+    }
+    const double variance = n_walks > 1 ? m2 / static_cast<double>(n_walks - 1) : 0.0;
+    if (out.mean) out.mean[p] = mean;
+    if (out.variance) out.variance[p] = variance;
+    if (out.standard_error) out.standard_error[p] = sqrt(variance / static_cast<double>(n_walks));
+    if (out.mean_steps) out.mean_steps[p] = steps / static_cast<double>(n_walks);
+    if (hits) atomicAdd(&ctr->max_steps_hits, hits);
+    atomicAdd(&ctr->total_steps, static_cast<unsigned long long>(steps));
+    atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n));
+}
+
 __global__ void merge_kernel(long long n_points, int chunks, int n_walks,
                              const uint8_t *__restrict__ location,
                              const TaskPartial *__restrict__ partials, Fields out,
@@ -267,22 +332,81 @@ __global__ void merge_kernel(long long n_points, int chunks, int n_walks,
     for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
          p < n_points; p += stride) {
         if (location[p] != 1) continue;
-        double n = 0.0, mean = 0.0, m2 = 0.0, steps = 0.0;
-        unsigned long long hits = 0;
-        for (int c = 0; c < chunks; ++c) {
-            const TaskPartial tp = partials[p * chunks + c];
-            chan_merge(n, mean, m2, tp.n, tp.mean, tp.m2);
-            steps += tp.steps;
-            hits += tp.hits;
+        merge_point(p, chunks, n_walks, partials, out, ctr);
+    }
+}
+
+// ------------------------------------------------------------------ batches
+
+__global__ void merge_batch_kernel(const BatchItem *__restrict__ items, int n_items,
+                                   long long n_points) {
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+         t < n_points; t += stride) {
+        int lo = 0, hi = n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].point_begin <= t) lo = mid;
+            else hi = mid - 1;
         }
-        const double variance = n_walks > 1 ? m2 / static_cast<double>(n_walks - 1) : 0.0;
-        if (out.mean) out.mean[p] = mean;
-        if (out.variance) out.variance[p] = variance;
-        if (out.standard_error) out.standard_error[p] = sqrt(variance / static_cast<double>(n_walks));
-        if (out.mean_steps) out.mean_steps[p] = steps / static_cast<double>(n_walks);
-        if (hits) atomicAdd(&ctr->max_steps_hits, hits);
-        atomicAdd(&ctr->total_steps, static_cast<unsigned long long>(steps));
-        atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n));
+        const BatchItem &it = items[lo];
+        const long long p = t - it.point_begin;
+        if (it.a.location[p] != 1) continue;
+        merge_point(p, it.a.chunks, it.a.n_walks, it.a.partials, it.out, it.a.ctr);
+    }
+}
+
+template <int DIM, class Eq>
+cudaError_t batch_typed(int precision, const BatchItem *items, int n_items, long long n_tasks,
+                        unsigned long long *queue, int blocks, cudaStream_t stream) {
+    if (precision == 32) {
+        walk_batch_kernel<DIM, Eq, float, 3><<<blocks, 256, 0, stream>>>(items, n_items, n_tasks,
+                                                                         queue);
+    } else {
+        walk_batch_kernel<DIM, Eq, double, 1><<<blocks, 256, 0, stream>>>(items, n_items,
+                                                                          n_tasks, queue);
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM, class Eq>
+cudaError_t batch_blocks_typed(int precision, int &blocks) {
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaError_t e = precision == 32
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &per_sm, walk_batch_kernel<DIM, Eq, float, 3>, 256, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &per_sm, walk_batch_kernel<DIM, Eq, double, 1>, 256, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    blocks = sms * (per_sm > 0 ? per_sm : 1);
+    return cudaSuccess;
+}
+
+template <int DIM>
+cudaError_t batch_dispatch(int kind, int precision, const BatchItem *items, int n_items,
+                           long long n_tasks, unsigned long long *queue, int blocks,
+                           cudaStream_t stream, int *blocks_out) {
+    switch (kind) {
+        case kLaplace:
+            return blocks_out ? batch_blocks_typed<DIM, Laplace<DIM>>(precision, *blocks_out)
+                              : batch_typed<DIM, Laplace<DIM>>(precision, items, n_items, n_tasks,
+                                                               queue, blocks, stream);
+        case kPoisson:
+            return blocks_out ? batch_blocks_typed<DIM, Poisson<DIM>>(precision, *blocks_out)
+                              : batch_typed<DIM, Poisson<DIM>>(precision, items, n_items, n_tasks,
+                                                               queue, blocks, stream);
+        case kScreened:
+            return blocks_out ? batch_blocks_typed<DIM, Screened<DIM>>(precision, *blocks_out)
+                              : batch_typed<DIM, Screened<DIM>>(precision, items, n_items,
+                                                                n_tasks, queue, blocks, stream);
+        default:
+            return blocks_out ? batch_blocks_typed<DIM, Helmholtz<DIM>>(precision, *blocks_out)
+                              : batch_typed<DIM, Helmholtz<DIM>>(precision, items, n_items,
+                                                                 n_tasks, queue, blocks, stream);
     }
 }
 
@@ -326,8 +450,28 @@ __global__ void closest32_kernel(SceneView s, WideView w, const double *pts, lon
     if (bid) bid[t] = b;
 }
 
+// The equation object of a descriptor, built on the host for kernel arguments.
+template <class Eq>
+Eq eq_host(const EqDesc &e);
+template <>
+Laplace<2> eq_host(const EqDesc &) { return Laplace<2>{}; }
+template <>
+Laplace<3> eq_host(const EqDesc &) { return Laplace<3>{}; }
+template <>
+Poisson<2> eq_host(const EqDesc &e) { return Poisson<2>{e.mode, e.alpha}; }
+template <>
+Poisson<3> eq_host(const EqDesc &e) { return Poisson<3>{e.mode, e.alpha}; }
+template <>
+Screened<2> eq_host(const EqDesc &e) { return Screened<2>{e.mode, e.alpha}; }
+template <>
+Screened<3> eq_host(const EqDesc &e) { return Screened<3>{e.mode, e.alpha}; }
+template <>
+Helmholtz<2> eq_host(const EqDesc &) { return Helmholtz<2>{}; }
+template <>
+Helmholtz<3> eq_host(const EqDesc &) { return Helmholtz<3>{}; }
+
 template <int DIM, class Eq>
-cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
+cudaError_t launch_fast_typed(const FastArgs &a, const EqDesc &e, int precision,
                               const FastPlan &plan, cudaStream_t stream) {
     // persistent grid: every block that can be resident at once (plan.blocks
     // overrides when positive)
@@ -337,13 +481,13 @@ cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
             return cudaSuccess;
         }
         int per_sm = 0, dev = 0, sms = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
-                                                                      plan.threads, smem);
-        if (e != cudaSuccess) return e;
-        e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return e;
+        cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                                        plan.threads, smem);
+        if (err != cudaSuccess) return err;
+        err = cudaGetDevice(&dev);
+        if (err != cudaSuccess) return err;
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (err != cudaSuccess) return err;
         blocks = sms * (per_sm > 0 ? per_sm : 1);
         return cudaSuccess;
     };
@@ -351,18 +495,18 @@ cudaError_t launch_fast_typed(const FastArgs &a, const Eq &eq, int precision,
     if (precision == 32) {
         auto k = walk_fast_kernel<DIM, Eq, float, 3>;
         if (plan.smem_bytes > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 plan.smem_bytes);
-            if (e != cudaSuccess) return e;
+            cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   plan.smem_bytes);
+            if (err != cudaSuccess) return err;
         }
-        cudaError_t e = grid_for(k, plan.smem_bytes, blocks);
-        if (e != cudaSuccess) return e;
-        k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq);
+        cudaError_t err = grid_for(k, plan.smem_bytes, blocks);
+        if (err != cudaSuccess) return err;
+        k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq_host<Eq>(e));
     } else {
         auto k = walk_fast_kernel<DIM, Eq, double, 1>;
-        cudaError_t e = grid_for(k, 0, blocks);
-        if (e != cudaSuccess) return e;
-        k<<<blocks, plan.threads, 0, stream>>>(a, eq);
+        cudaError_t err = grid_for(k, 0, blocks);
+        if (err != cudaSuccess) return err;
+        k<<<blocks, plan.threads, 0, stream>>>(a, eq_host<Eq>(e));
     }
     return cudaGetLastError();
 }
@@ -372,15 +516,13 @@ cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const Fa
                             cudaStream_t stream) {
     switch (e.kind) {
         case kLaplace:
-            return launch_fast_typed<DIM>(a, Laplace<DIM>{}, precision, plan, stream);
+            return launch_fast_typed<DIM, Laplace<DIM>>(a, e, precision, plan, stream);
         case kPoisson:
-            return launch_fast_typed<DIM>(a, Poisson<DIM>{e.mode, e.alpha}, precision, plan,
-                                          stream);
+            return launch_fast_typed<DIM, Poisson<DIM>>(a, e, precision, plan, stream);
         case kScreened:
-            return launch_fast_typed<DIM>(a, Screened<DIM>{e.mode, e.alpha}, precision, plan,
-                                          stream);
+            return launch_fast_typed<DIM, Screened<DIM>>(a, e, precision, plan, stream);
         default:
-            return launch_fast_typed<DIM>(a, Helmholtz<DIM>{}, precision, plan, stream);
+            return launch_fast_typed<DIM, Helmholtz<DIM>>(a, e, precision, plan, stream);
     }
 }
 
@@ -408,14 +550,10 @@ FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, in
     return p;
 }
 
-cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointSet &ps,
-                             uint64_t seed, EqDesc eq,
-                             int n_walks, double epsilon, int max_steps, double shell_delta,
-                             int precision, const FastPlan &plan, const uint8_t *location,
-                             const StartRecord *start, TaskPartial *partials,
-                             unsigned long long *queue, Fields out, DeviceCounters *counters,
-                             cudaStream_t stream, cudaEvent_t after_walk) {
-    if (ps.n <= 0) return cudaSuccess;
+FastArgs make_fast_args(const SceneView &s, const WideView &w, const PointSet &ps, uint64_t seed,
+                        int n_walks, double epsilon, int max_steps, double shell_delta,
+                        const FastPlan &plan, const uint8_t *location, const StartRecord *start,
+                        TaskPartial *partials, unsigned long long *queue, DeviceCounters *ctr) {
     FastArgs a{};
     a.s = s;
     a.ps = ps;
@@ -428,9 +566,9 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
     a.chunks = plan.chunks;
     a.n_tasks = plan.n_tasks;
     a.w = w;
-    a.stage = plan.stage_scene ? 1 : 0;
-    a.stage_box = plan.stage_scene ? w.box_total : 0;
-    a.stage_prim = plan.stage_prims ? (w.dim == 2 ? 5 : 16) * w.npad : 0;
+    a.stage = 0;
+    a.stage_box = 0;
+    a.stage_prim = 0;
     // FP32 queries are conservative to a relative tau = 2^-10 outside the
     // epsilon shell and exact inside it (see Nearest32)
     const double tau = 1.0 / 1024.0;
@@ -443,7 +581,23 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
     a.start = start;
     a.partials = partials;
     a.queue = queue;
-    a.ctr = counters;
+    a.ctr = ctr;
+    return a;
+}
+
+cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointSet &ps,
+                             uint64_t seed, EqDesc eq,
+                             int n_walks, double epsilon, int max_steps, double shell_delta,
+                             int precision, const FastPlan &plan, const uint8_t *location,
+                             const StartRecord *start, TaskPartial *partials,
+                             unsigned long long *queue, Fields out, DeviceCounters *counters,
+                             cudaStream_t stream, cudaEvent_t after_walk) {
+    if (ps.n <= 0) return cudaSuccess;
+    FastArgs a = make_fast_args(s, w, ps, seed, n_walks, epsilon, max_steps, shell_delta, plan,
+                                location, start, partials, queue, counters);
+    a.stage = plan.stage_scene ? 1 : 0;
+    a.stage_box = plan.stage_scene ? w.box_total : 0;
+    a.stage_prim = plan.stage_prims ? (w.dim == 2 ? 5 : 16) * w.npad : 0;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
     e = s.dim == 2 ? launch_fast_dim<2>(a, eq, precision, plan, stream)
@@ -457,6 +611,30 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
     if (b < 1) b = 1;
     merge_kernel<<<static_cast<int>(b), 256, 0, stream>>>(ps.n, plan.chunks, n_walks, location,
                                                         partials, out, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_walk_blocks(int dim, int kind, int precision, int *blocks) {
+    return dim == 2 ? batch_dispatch<2>(kind, precision, nullptr, 0, 0, nullptr, 0, nullptr, blocks)
+                    : batch_dispatch<3>(kind, precision, nullptr, 0, 0, nullptr, 0, nullptr, blocks);
+}
+
+cudaError_t launch_walk_batch(int dim, int kind, int precision, const BatchItem *items,
+                              int n_items, long long n_tasks, unsigned long long *queue,
+                              int blocks, cudaStream_t stream) {
+    if (n_items <= 0 || n_tasks <= 0) return cudaSuccess;
+    return dim == 2 ? batch_dispatch<2>(kind, precision, items, n_items, n_tasks, queue, blocks,
+                                        stream, nullptr)
+                    : batch_dispatch<3>(kind, precision, items, n_items, n_tasks, queue, blocks,
+                                        stream, nullptr);
+}
+
+cudaError_t launch_merge_batch(const BatchItem *items, int n_items, long long n_points,
+                               cudaStream_t stream) {
+    if (n_items <= 0 || n_points <= 0) return cudaSuccess;
+    long long b = (n_points + 255) / 256;
+    if (b > 148 * 64) b = 148 * 64;
+    merge_batch_kernel<<<static_cast<int>(b), 256, 0, stream>>>(items, n_items, n_points);
     return cudaGetLastError();
 }
 

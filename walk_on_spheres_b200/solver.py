@@ -15,6 +15,7 @@ All work runs in the CUDA library; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -58,6 +59,7 @@ class Solver:
         ctx = C.c_void_p()
         _lib.check(self._L.wos_context_create(device, C.byref(ctx)))
         self._ctx = ctx
+        self._batches = weakref.WeakSet()
         self.device = device
         self.dim = 0
         self.n_prims = 0
@@ -65,6 +67,8 @@ class Solver:
 
     def close(self):
         if self._ctx:
+            for b in list(self._batches):
+                b.close()
             self._L.wos_context_destroy(self._ctx)
             self._ctx = None
 
