@@ -22,6 +22,12 @@ With N GPUs (torchrun, one process per GPU over NCCL) every rank solves its
 own copy of the workload on a disjoint range of grid indices (weak scaling);
 the job time is the maximum over ranks.
 
+The line also carries `adjoint`: backward passes per second of the
+differentiable heat-source workload (3D Gaussian source on a 0.10 x 0.05 x
+0.01 m slab of ~20k triangles, 4096 interior probes, 2048 walks; each pass
+replays the forward walks from their seeds and returns the gradient with
+respect to Q, x0, sigma and every vertex value), timed the same way.
+
 `--impl reference` times the reference's own CPU code (oracle/_ref, the
 reference sources compiled with one-rank stand-ins) on all host threads on a
 bounded sample of the same workload; under torchrun only rank 0 runs it.
@@ -61,6 +67,16 @@ BYTES_PER_QUERY = 1863.4
 # one-pass ncu capture of the full launch (profiles/walk_fast_kernel_poisson2d_
 # circle1024.md): 2.84 MB and 3.32 MB for the two source modes.
 TRAFFIC_BYTES_PER_LAUNCH = 3.08e6
+# Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
+# 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in
+# the interior, 2048 FP32 walks each; one "gradient" is one full backward
+# pass (the vector-Jacobian product of the 4096 probe values with respect to
+# Q, x0, sigma and every vertex value).
+ADJ_WORKLOAD = "heat3d_slab20k_4096probes"
+ADJ_PROBES = 4096
+ADJ_WALKS = 2048
+ADJ_EPSILON = 1e-5
+ADJ_THETA = (1e3, (0.05, 0.025, 0.01), 2e-3)
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -77,6 +93,8 @@ def parse():
                     help="CPU budget of the baseline sample")
     ap.add_argument("--walks", type=int, default=N_WALKS,
                     help="walks per point (profiling of smaller cases; the headline uses 4096)")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint-gradient leg")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the device solves only (no matched-SE, e2e or CPU legs)")
     return ap.parse_args()
@@ -213,6 +231,48 @@ def reference_rate(budget_s: float, threads: int | None = None):
 
 
 # ---------------------------------------------------------------- GPU arm
+def adjoint_leg(solver, args, rank, world, dist, dev):
+    """Backward passes (adjoint replay) of the heat-source workload per second,
+    device time from the library's CUDA events, max over ranks."""
+    import torch
+    from walk_on_spheres_b200 import meshes
+    from walk_on_spheres_b200.heat import HeatProblem
+    slab = meshes.slab_box(target_triangles=20000)
+    solver.set_mesh(slab)
+    rng = np.random.default_rng(20240 + rank)
+    lo, hi = np.zeros(3), np.array([0.10, 0.05, 0.01])
+    probes = lo + (hi - lo) * rng.uniform(0.001, 0.999, size=(ADJ_PROBES, 3))
+    heat = HeatProblem(solver, probes, N_walks=ADJ_WALKS, epsilon=ADJ_EPSILON,
+                       seed=SEED + rank * 1000003, source_mode="green", method="fast")
+    g = np.zeros(heat.n_verts)
+    Q, x0, sigma = ADJ_THETA
+    fwd = heat.forward(Q, x0, sigma, g)
+    for _ in range(args.warmup):
+        heat.adjoint(Q, x0, sigma, g)
+    ms, walks, steps = [], 0, 0
+    for _ in range(args.steps):
+        r = heat.adjoint(Q, x0, sigma, g)
+        ms.append(r.counters["total_ms"])
+        walks += r.counters["total_walks"]
+        steps += r.counters["total_steps"]
+    dev_s = sum(ms) / 1000.0
+    if dist:
+        t = torch.tensor([dev_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s = float(t.item())
+        tw = torch.tensor([float(walks), float(steps)], dtype=torch.float64, device=dev)
+        dist.all_reduce(tw)
+        walks, steps = int(tw[0].item()), int(tw[1].item())
+    return {"workload": ADJ_WORKLOAD, "metric": "adjoint gradients/s",
+            "value": world * args.steps / dev_s, "unit": "gradients/s",
+            "gradient": f"VJP of {ADJ_PROBES} probe values w.r.t. Q, x0 (3), sigma and "
+                        f"{heat.n_verts} vertex values",
+            "backward_ms": dev_s * 1000.0 / args.steps, "forward_ms": fwd.counters["total_ms"],
+            "walks_per_s": walks / dev_s, "closest_point_queries_per_s": steps / dev_s,
+            "N_walks": ADJ_WALKS, "epsilon": ADJ_EPSILON, "method": "FAST_FP32",
+            "triangles": int(slab.prims.shape[0]), "gpu_launches_per_gradient": 3}
+
+
 def gpu_arm(args, rank, world, local):
     import torch
     from walk_on_spheres_b200 import Solver
@@ -390,6 +450,8 @@ def gpu_arm(args, rank, world, local):
         "clocks": clock,
         "wall_s_timed_region": wall,
     }
+    if not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(solver, args, rank, world, dist, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, desc, threads, _ = reference_rate(args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",

@@ -1,6 +1,6 @@
 """Throughput and accuracy of the single-solve workloads, per walk method.
 
-    python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0] [--tune]
     python -m walk_on_spheres_b200.benchmarks --batch [--scale 1.0]
 
 Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
@@ -73,15 +73,29 @@ def _coords(s: Solver, nx, ny, nz):
     return np.meshgrid(*ax, indexing="ij")
 
 
-def run(name: str, scale: float = 1.0, device: int = 0) -> dict:
+def run(name: str, scale: float = 1.0, device: int = 0, tune: bool = False) -> dict:
     w = WORKLOADS[name]
-    s = Solver(device).set_mesh(w["mesh"]())
+    mesh = w["mesh"]()
+    s = Solver(device).set_mesh(mesh)
     nx, ny, nz = w["grid"]
     walks = max(16, int(round(w["walks"] * scale)))
     out = {"workload": name, "walks": walks, "methods": {}}
+    tuned = None
+    if tune:
+        from .autotune import Tuner
+        tuned = Tuner(s).tune(mesh, w["eq"], (nx, ny, nz), N_walks=walks, method="fast",
+                              **w["kw"])
+        out["tuning"] = {"chunk": tuned.chunk, "blocks": tuned.blocks,
+                         "leaf_size": tuned.leaf_size,
+                         "probe_walks_per_s": tuned.walks_per_s,
+                         "candidates": [{k: r[k] for k in ("leaf_size", "chunk", "blocks",
+                                                             "walks_per_s")}
+                                        for r in tuned.table]}
     res = {}
     for method in ("fast", "fast64", "plain"):
         n = walks if method != "plain" else min(walks, w.get("plain_walks", walks))
+        if tuned is not None and method != "fast":
+            s.set_tuning(0, 0)
         r = s.solve_grid(w["eq"], nx, ny, nz, N_walks=n, method=method, **w["kw"])
         c = r.counters
         secs = c["walk_ms"] / 1000.0
@@ -214,6 +228,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workloads", default=",".join(WORKLOADS))
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--tune", action="store_true",
+                    help="autotune the FAST_FP32 schedule and leaf size first")
     ap.add_argument("--batch", action="store_true",
                     help="run the 64-solve mixed batch instead of the single solves")
     a = ap.parse_args(argv)
@@ -221,7 +237,7 @@ def main(argv=None) -> int:
         print(json.dumps(run_batch(a.scale, a.device)), flush=True)
         return 0
     for name in a.workloads.split(","):
-        print(json.dumps(run(name.strip(), a.scale, a.device)), flush=True)
+        print(json.dumps(run(name.strip(), a.scale, a.device, a.tune)), flush=True)
     return 0
 
 

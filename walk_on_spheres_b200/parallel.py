@@ -40,9 +40,14 @@ def shard_bounds(n: int, rank: int, world: int) -> tuple[int, int]:
 def grid_points(grid, dim: int, start: int, end: int) -> np.ndarray:
     """Coordinates of linear indices [start, end) of `grid`, computed like
     grid_coordinate (include/wos/grid.hpp:12-18): min + (max-min)*i/(N-1)."""
+    return grid_coords(grid, dim, np.arange(start, end, dtype=np.int64))
+
+
+def grid_coords(grid, dim: int, lin) -> np.ndarray:
+    """Coordinates of the given linear indices of `grid` (row-major i, j, k)."""
     nx, ny = int(grid.Nx), int(grid.Ny)
     nz = int(grid.Nz) if dim == 3 else 1
-    lin = np.arange(start, end, dtype=np.int64)
+    lin = np.asarray(lin, dtype=np.int64)
     i, j, k = lin // (ny * nz), (lin // nz) % ny, lin % nz
 
     def coord(lo, hi, idx, count):
