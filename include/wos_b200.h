@@ -41,8 +41,12 @@ enum {
     WOS_EQ_HELMHOLTZ = 3
 };
 
-/* Source sampling modes (include/wos/source_mode.hpp:5-9). */
-enum { WOS_SOURCE_UNIFORM = 0, WOS_SOURCE_GREEN = 1 };
+/* Source sampling modes (include/wos/source_mode.hpp:5-9).  WOS_SOURCE_MIS is
+ * the reference's GreenSourceMIS (include/wos/source_sampling.hpp:35-78): it
+ * needs a source proposal, which only the Gaussian heat source below
+ * provides; the registry equations reject it, as the reference's walk does
+ * (include/wos/wos.hpp:83-92). */
+enum { WOS_SOURCE_UNIFORM = 0, WOS_SOURCE_GREEN = 1, WOS_SOURCE_MIS = 2 };
 
 /* Walk methods.
  *  PLAIN_FP64: the reference estimator (include/wos/wos.hpp:54-191) in FP64,
@@ -248,6 +252,16 @@ typedef struct {
     double Q;       /* amplitude */
     double x0[3];   /* centre (x0[2] unused in 2D) */
     double sigma;   /* width (> 0) */
+    /* WOS_SOURCE_MIS only: each step draws its source point from the Green
+     * density of the ball with this probability, else from the proposal
+     * N(proposal_x0, proposal_sigma^2 / 2 I) (the source's own shape), and
+     * weighs it by the balance heuristic G f / (beta p_green + (1 - beta)
+     * p_proposal), as include/wos/source_sampling.hpp:35-78 does.  The
+     * proposal is held fixed under differentiation; proposal_sigma <= 0
+     * takes x0 and sigma. */
+    double mis_green_probability;
+    double proposal_x0[3];
+    double proposal_sigma;
 } wos_gaussian_source;
 
 /* Number of vertices of the current mesh (the length of the per-vertex
@@ -259,7 +273,7 @@ int wos_mesh_vertex_count(const wos_context *ctx, int *n_verts);
  * of include/wos/poisson.hpp:12-51) for the source above.  vertex_values:
  * host array of n_verts boundary values (NULL: g = 0).  params: N_walks,
  * epsilon (used as given), max_steps, max_ray_attempts, seed, source_mode
- * (uniform / Green source samples) and method (FAST_FP32 or FAST_FP64;
+ * (uniform, Green or MIS source samples) and method (FAST_FP32 or FAST_FP64;
  * PLAIN_FP64 is rejected); params->equation and alpha are ignored.  Probe i
  * is seeded like grid index point_index[i] (NULL: i).  Outputs as
  * wos_solve_points (host arrays, any may be NULL); boundary probes get

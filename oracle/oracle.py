@@ -354,8 +354,11 @@ class Oracle(_Lib):
     def heat_solve(self, mesh, probes, Q: float, x0, sigma: float, vertex_values=None,
                    weights=None, N_walks: int = 256, epsilon: float = 1e-3,
                    max_steps: int = 10000, max_ray_attempts: int = 12, seed: int = 0,
-                   source_mode: int = 1, point_index=None, n_threads: int = 0) -> dict:
-        """FP64 Gaussian heat-source walks (wo_heat_solve): per-probe mean, standard error,
+                   source_mode: int = 1, point_index=None, n_threads: int = 0,
+                   mis_green_probability: float = 0.5, proposal=None) -> dict:
+        """FP64 Gaussian heat-source walks (wo_heat_solve; source_mode 0 uniform, 1 Green, 2
+        Green-source MIS with probability `mis_green_probability` of a Green sample and the
+        proposal (x0, sigma) given or the source's own): per-probe mean, standard error,
         derivative means / standard errors du/d(Q, x0.x, x0.y, x0.z, sigma), locations and
         grad_vertex = sum_i weights[i] du_i/dg_v."""
         pts = np.ascontiguousarray(probes, dtype=np.float64).reshape(-1, mesh.dim)
@@ -369,6 +372,11 @@ class Oracle(_Lib):
         src.Q, src.sigma = float(Q), float(sigma)
         xs = list(np.asarray(x0, dtype=np.float64).ravel()) + [0.0, 0.0, 0.0]
         src.x0 = (C.c_double * 3)(*xs[:3])
+        src.mis_green_probability = float(mis_green_probability)
+        if proposal is not None:
+            pxs = list(np.asarray(proposal[0], dtype=np.float64).ravel()) + [0.0, 0.0, 0.0]
+            src.proposal_x0 = (C.c_double * 3)(*pxs[:3])
+            src.proposal_sigma = float(proposal[1])
         g = None if vertex_values is None else np.ascontiguousarray(vertex_values, np.float64)
         w = None if weights is None else np.ascontiguousarray(weights, np.float64)
         out = {"mean": np.zeros(n), "standard_error": np.zeros(n),
@@ -386,4 +394,6 @@ class Oracle(_Lib):
 
 
 class _Gaussian(C.Structure):
-    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double)]
+    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double),
+                ("mis_green_probability", C.c_double), ("proposal_x0", C.c_double * 3),
+                ("proposal_sigma", C.c_double)]

@@ -1592,7 +1592,51 @@ static double heat_source(const heat_job *job, const double p[3], double R, xosh
     const wo_gaussian *s = job->src;
     double y[3] = {0.0, 0.0, 0.0};
     double m;
-    if (job->pb->source_mode == 1) {
+    if (job->pb->source_mode == 2) {
+        /* include/wos/source_sampling.hpp:35-78: random mixture of the Green
+         * density and the Gaussian proposal, balance-heuristic weight */
+        const double beta = s->mis_green_probability;
+        const int own = !(s->proposal_sigma > 0.0);
+        const double *c = own ? s->x0 : s->proposal_x0;
+        const double ps = own ? s->sigma : s->proposal_sigma;
+        if (rng_unit(rng) < beta) {
+            const double radius =
+                d == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
+            if (d == 2) {
+                const double angle = 2.0 * M_PI * rng_unit(rng);
+                y[0] = p[0] + radius * cos(angle);
+                y[1] = p[1] + radius * sin(angle);
+            } else {
+                const double z = 2.0 * rng_unit(rng) - 1.0;
+                const double angle = 2.0 * M_PI * rng_unit(rng);
+                const double xy = sqrt(1.0 - z * z);
+                y[0] = p[0] + radius * xy * cos(angle);
+                y[1] = p[1] + radius * xy * sin(angle);
+                y[2] = p[2] + radius * z;
+            }
+        } else {
+            const double sc = ps / sqrt(2.0);
+            const double rho0 = sqrt(-2.0 * log(rng_unit_open(rng)));
+            const double a0 = 2.0 * M_PI * rng_unit(rng);
+            y[0] = c[0] + sc * rho0 * cos(a0);
+            y[1] = c[1] + sc * rho0 * sin(a0);
+            if (d == 3) {
+                const double rho1 = sqrt(-2.0 * log(rng_unit_open(rng)));
+                y[2] = c[2] + sc * rho1 * cos(2.0 * M_PI * rng_unit(rng));
+            }
+        }
+        const double r = dist3(p, y, d);
+        if (!(r > 0.0 && r < R)) return 0.0;
+        const double G = d == 2 ? pg_green_2d(R, r) : pg_green_3d(R, r);
+        const double mass = d == 2 ? pg_mass_2d(R) : pg_mass_3d(R);
+        double qq = 0.0;
+        for (int k = 0; k < d; ++k) qq += (y[k] - c[k]) * (y[k] - c[k]);
+        const double norm = 1.0 / (pow(M_PI, 0.5 * d) * pow(ps, d));
+        const double src_pdf = norm * exp(-qq / (ps * ps));
+        const double mix = beta * (G / mass) + (1.0 - beta) * src_pdf;
+        if (!(mix > 0.0)) return 0.0;
+        m = G / mix;
+    } else if (job->pb->source_mode == 1) {
         const double radius = d == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
         if (d == 2) {
             const double angle = 2.0 * M_PI * rng_unit(rng);
@@ -1737,6 +1781,10 @@ int wo_heat_solve(const wo_problem *pb, const wo_gaussian *src, const double *ve
                   unsigned char *location, double *grad_vertex) {
     if (pb->dim != 2 && pb->dim != 3) return 1;
     if (!(src->sigma > 0.0)) return 1;
+    if (pb->source_mode == 2 &&
+        !(src->mis_green_probability > 0.0 && src->mis_green_probability < 1.0)) {
+        return 1;
+    }
     bvh_t t;
     bvh_build(&t, pb);
     heat_job job;

@@ -114,6 +114,9 @@ typedef struct {
     double Q;
     double x0[3];
     double sigma;
+    double mis_green_probability;  /* source_mode 2 */
+    double proposal_x0[3];         /* proposal N(proposal_x0, proposal_sigma^2/2 I); */
+    double proposal_sigma;         /* <= 0: x0 and sigma */
 } wo_gaussian;
 
 /* FP64 heat-source walks at `n` probes (host n*dim; probe i seeded like grid
@@ -122,7 +125,7 @@ typedef struct {
  * sigma) and their standard errors (n*5), the location code, and
  * grad_vertex[v] = sum_i weights[i] du_i/dg_v (weights NULL: all 1).  Uses
  * pb's mesh, N_walks, epsilon, max_steps, max_ray_attempts, seed,
- * source_mode and n_threads.  Any output may be NULL.  Returns 0 on
+ * source_mode (0 uniform, 1 Green, 2 Green-source MIS) and n_threads.  Any output may be NULL.  Returns 0 on
  * success. */
 int wo_heat_solve(const wo_problem *pb, const wo_gaussian *src, const double *vertex_values,
                   const double *probes, long long n, const double *weights, double *mean,

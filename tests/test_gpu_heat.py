@@ -1,5 +1,7 @@
 """GPU heat source and its adjoint (kernels_adjoint.cu through the C ABI).
 
+Source modes: uniform, Green and Green-source MIS.
+
 Tolerances:
 * replay: the adjoint's replayed probe values equal the forward's bit for
   bit (same kernel, same seeds).
@@ -59,9 +61,11 @@ def test_adjoint_replays_forward_bit_for_bit(solver, slab_mesh, method):
     assert f.counters["total_steps"] == a.counters["total_steps"]
 
 
-@pytest.mark.parametrize("mode", ["uniform", "green"])
+@pytest.mark.parametrize("mode", ["uniform", "green", "mis"])
 def test_adjoint_matches_crn_central_differences(solver, slab_mesh, mode):
-    heat = _heat(solver, slab_mesh, _slab_probes(96, seed=2), source_mode=mode)
+    # the MIS proposal is held fixed while the source parameters move
+    heat = _heat(solver, slab_mesh, _slab_probes(96, seed=2), source_mode=mode,
+                 proposal=(SLAB_X0, 2e-3))
     a = heat.adjoint(THETA[0], THETA[1:4], THETA[4])
     for k in range(5):
         h = 1e-4 * abs(THETA[k])
@@ -93,15 +97,18 @@ def test_adjoint_is_linear_in_vertex_values(solver, slab_mesh):
     assert np.allclose(a.grad_source, w @ a.jacobian, rtol=1e-9, atol=0)
 
 
-@pytest.mark.parametrize("method", ["fast", "fast64"])
-def test_heat_matches_fp64_oracle(solver, oracle, slab_mesh, method):
+@pytest.mark.parametrize("method,mode", [("fast", "green"), ("fast64", "green"),
+                                         ("fast", "mis")])
+def test_heat_matches_fp64_oracle(solver, oracle, slab_mesh, method, mode):
     probes = _slab_probes(48, seed=5)
     g = np.random.default_rng(3).uniform(0.0, 1.0, size=slab_mesh.verts.shape[0])
-    heat = _heat(solver, slab_mesh, probes, N_walks=4096, method=method, seed=21)
+    heat = _heat(solver, slab_mesh, probes, N_walks=4096, method=method, seed=21,
+                 source_mode=mode)
     f = heat.forward(THETA[0], THETA[1:4], THETA[4], g)
     a = heat.adjoint(THETA[0], THETA[1:4], THETA[4], g)
     ref = oracle.heat_solve(slab_mesh, probes, THETA[0], THETA[1:4], THETA[4], vertex_values=g,
-                            N_walks=4096, epsilon=1e-5, seed=21, source_mode=1, n_threads=8)
+                            N_walks=4096, epsilon=1e-5, seed=21,
+                            source_mode={"green": 1, "mis": 2}[mode], n_threads=8)
     assert np.array_equal(f.location, ref["location"])
     z = (f.mean - ref["mean"]) / np.hypot(f.standard_error, ref["standard_error"])
     assert (np.abs(z) <= 4.5).mean() >= 0.97, np.abs(z).max()
@@ -112,8 +119,9 @@ def test_heat_matches_fp64_oracle(solver, oracle, slab_mesh, method):
         assert (np.abs(zk) <= 4.5).mean() >= 0.97, (k, np.abs(zk).max())
 
 
+@pytest.mark.parametrize("mode", ["green", "mis"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_heat_centre_value_matches_quadrature(solver, dim):
+def test_heat_centre_value_matches_quadrature(solver, dim, mode):
     from walk_on_spheres_b200.heat import HeatProblem
     if dim == 2:
         mesh, x0 = meshes.circle(segments=1024), (0.2, -0.1)
@@ -122,7 +130,8 @@ def test_heat_centre_value_matches_quadrature(solver, dim):
     Q, sigma = 2.0, 0.3
     ref = centre_value(dim, 1.0, Q, x0, sigma)
     solver.set_mesh(mesh)
-    heat = HeatProblem(solver, np.zeros((1, dim)), N_walks=200000, epsilon=1e-4, seed=8)
+    heat = HeatProblem(solver, np.zeros((1, dim)), N_walks=200000, epsilon=1e-4, seed=8,
+                       source_mode=mode)
     a = heat.adjoint(Q, x0, sigma)
     f = heat.forward(Q, x0, sigma)
     assert f.location[0] == 1
@@ -194,3 +203,26 @@ def test_autograd_function_matches_crn_differences(solver, slab_mesh):
     h = 1e-3
     fd = (L(THETA, g0 + h * d) - L(THETA, g0 - h * d)) / (2 * h)
     assert abs(float(g.grad.numpy() @ d) - fd) <= 1e-6 * abs(fd)
+
+
+def test_mis_narrow_source_and_registry_rejection(solver):
+    """MIS against Green sampling for a source much narrower than the balls
+    around it (standard error several times smaller, same mean), and the
+    registry equations' rejection of MIS (they have no source proposal, as in
+    include/wos/wos.hpp:83-92)."""
+    from walk_on_spheres_b200._lib import WosError
+    from walk_on_spheres_b200.heat import HeatProblem
+    solver.set_mesh(meshes.circle(segments=1024))
+    ref = centre_value(2, 1.0, 2.0, (0.2, -0.1), 0.05)
+    out = {}
+    for mode in ("green", "mis"):
+        heat = HeatProblem(solver, np.zeros((1, 2)), N_walks=100000, epsilon=1e-4, seed=5,
+                           source_mode=mode)
+        out[mode] = heat.forward(2.0, (0.2, -0.1), 0.05)
+    assert out["mis"].standard_error[0] < out["green"].standard_error[0] / 3
+    assert abs(out["mis"].mean[0] - ref["u"]) <= 4 * out["mis"].standard_error[0] + 2e-3 * ref["u"]
+    with pytest.raises(WosError, match="GreenSourceMIS"):
+        solver.solve_grid("poisson", 8, 8, N_walks=16, source_mode="mis", method="fast")
+    with pytest.raises(WosError, match="MIS probability"):
+        HeatProblem(solver, np.zeros((1, 2)), N_walks=16, source_mode="mis",
+                    mis_green_probability=1.0).forward(2.0, (0.2, -0.1), 0.05)

@@ -3,6 +3,9 @@ against common-random-number central differences of its own forward values,
 exact linearity in the per-vertex boundary data, and quadrature references
 at the centre of a disk and a ball.
 
+Source modes: uniform, Green and Green-source MIS (with the source's own
+Gaussian as proposal).
+
 Tolerances:
 * CRN central differences (h = 1e-4 relative to each parameter, FP64 walks,
   same seeds): the walks are identical, so the difference quotient and the
@@ -37,10 +40,12 @@ def _slab_probes(n, seed=0):
     return p
 
 
-@pytest.mark.parametrize("mode", [0, 1], ids=["uniform", "green"])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["uniform", "green", "mis"])
 def test_oracle_derivatives_match_crn_differences(oracle, slab, mode):
     probes = _slab_probes(6)
-    base = dict(N_walks=200, epsilon=1e-5, seed=11, source_mode=mode, n_threads=4)
+    # the MIS proposal stays fixed while the source parameters move
+    base = dict(N_walks=200, epsilon=1e-5, seed=11, source_mode=mode, n_threads=4,
+                proposal=(SLAB_X0, 2e-3))
     theta = np.array([1e3, *SLAB_X0, 2e-3])
     r = oracle.heat_solve(slab, probes, theta[0], theta[1:4], theta[4], **base)
     assert (r["location"] == 1).all()
@@ -72,8 +77,9 @@ def test_oracle_is_linear_in_vertex_values(oracle, slab):
     assert abs(with_g["grad_vertex"].sum() - w.sum()) <= 1e-12 * np.abs(w).sum()
 
 
+@pytest.mark.parametrize("mode", [1, 2], ids=["green", "mis"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_oracle_centre_value_matches_quadrature(oracle, dim):
+def test_oracle_centre_value_matches_quadrature(oracle, dim, mode):
     if dim == 2:
         mesh = meshes.circle(segments=1024)
         x0, N = (0.2, -0.1), 6000
@@ -83,9 +89,22 @@ def test_oracle_centre_value_matches_quadrature(oracle, dim):
     Q, sigma = 2.0, 0.3
     ref = centre_value(dim, 1.0, Q, x0, sigma)
     r = oracle.heat_solve(mesh, np.zeros((1, dim)), Q, x0, sigma, N_walks=N, epsilon=1e-4,
-                          seed=4, source_mode=1, n_threads=8)
+                          seed=4, source_mode=mode, n_threads=8)
     assert r["location"][0] == 1
     assert abs(r["mean"][0] - ref["u"]) <= 4 * r["standard_error"][0] + 2e-3 * abs(ref["u"])
     for k in [0, 1, 2, 4] + ([3] if dim == 3 else []):
         err = abs(r["jacobian"][0, k] - ref["jacobian"][k])
         assert err <= 4 * r["jacobian_se"][0, k] + 2e-3 * np.abs(ref["jacobian"]).max(), k
+
+
+def test_oracle_mis_reduces_variance_for_a_narrow_source(oracle):
+    """Green-source MIS (include/wos/source_sampling.hpp:35-78) with the source's
+    own Gaussian as proposal: for a source much narrower than the balls that
+    contain it, Green sampling rarely lands on it; the mixture does."""
+    mesh = meshes.circle(segments=1024)
+    kw = dict(N_walks=20000, epsilon=1e-4, seed=6, n_threads=8)
+    ref = centre_value(2, 1.0, 2.0, (0.2, -0.1), 0.05)
+    green = oracle.heat_solve(mesh, np.zeros((1, 2)), 2.0, (0.2, -0.1), 0.05, source_mode=1, **kw)
+    mis = oracle.heat_solve(mesh, np.zeros((1, 2)), 2.0, (0.2, -0.1), 0.05, source_mode=2, **kw)
+    assert mis["standard_error"][0] < green["standard_error"][0] / 3
+    assert abs(mis["mean"][0] - ref["u"]) <= 4 * mis["standard_error"][0] + 2e-3 * ref["u"]

@@ -52,8 +52,11 @@ class Counters(C.Structure):
 
 
 class GaussianSource(C.Structure):
-    """wos_gaussian_source: f(x) = Q exp(-|x - x0|^2 / sigma^2)."""
-    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double)]
+    """wos_gaussian_source: f(x) = Q exp(-|x - x0|^2 / sigma^2), plus the MIS mixture
+    probability and proposal."""
+    _fields_ = [("Q", C.c_double), ("x0", C.c_double * 3), ("sigma", C.c_double),
+                ("mis_green_probability", C.c_double), ("proposal_x0", C.c_double * 3),
+                ("proposal_sigma", C.c_double)]
 
 
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,

@@ -259,7 +259,12 @@ static std::string check_params(const wos_context *ctx, const wos_params *p) {
     if (!p) return "null params";
     if (!ctx->has_mesh) return "no mesh uploaded";
     if (p->equation < 0 || p->equation > 3) return "unknown equation kind";
-    if (p->source_mode != 0 && p->source_mode != 1) return "source_mode must be 0 or 1";
+    if (p->source_mode == WOS_SOURCE_MIS &&
+        (p->equation == WOS_EQ_POISSON || p->equation == WOS_EQ_SCREENED_POISSON)) {
+        // include/wos/wos.hpp:83-92: no registry equation has a source proposal
+        return "GreenSourceMIS requires a source proposal sampler and PDF";
+    }
+    if (p->source_mode < 0 || p->source_mode > 2) return "source_mode must be 0, 1 or 2";
     if (p->N_walks < 1) return "N_walks must be >= 1";
     if (!(p->epsilon > 0.0) || !std::isfinite(p->epsilon)) return "epsilon must be positive";
     if (p->max_steps < 1) return "max_steps must be >= 1";

@@ -20,7 +20,7 @@
 namespace wosb {
 
 enum : int { kLaplace = 0, kPoisson = 1, kScreened = 2, kHelmholtz = 3 };
-enum : int { kUniform = 0, kGreen = 1 };
+enum : int { kUniform = 0, kGreen = 1, kMis = 2 };
 
 template <typename T>
 struct V3 {

@@ -84,7 +84,7 @@ std::string check_heat(const wos_context *ctx, const wos_params *p,
     if (!p) return "null params";
     if (!ctx->has_mesh) return "no mesh uploaded";
     if (!s) return "null source";
-    if (p->source_mode != 0 && p->source_mode != 1) return "source_mode must be 0 or 1";
+    if (p->source_mode < 0 || p->source_mode > 2) return "source_mode must be 0, 1 or 2";
     if (p->N_walks < 1) return "N_walks must be >= 1";
     if (!(p->epsilon > 0.0) || !std::isfinite(p->epsilon)) return "epsilon must be positive";
     if (p->max_steps < 1) return "max_steps must be >= 1";
@@ -96,6 +96,18 @@ std::string check_heat(const wos_context *ctx, const wos_params *p,
     if (!std::isfinite(s->Q) || !std::isfinite(s->x0[0]) || !std::isfinite(s->x0[1]) ||
         !std::isfinite(s->x0[2])) {
         return "source parameters must be finite";
+    }
+    if (p->source_mode == WOS_SOURCE_MIS) {
+        // include/wos/source_sampling.hpp:44-48
+        const double b = s->mis_green_probability;
+        if (!(b > 0.0 && b < 1.0) || !std::isfinite(b)) {
+            return "Green-source MIS probability must be finite and in (0, 1)";
+        }
+        if (s->proposal_sigma > 0.0 &&
+            (!std::isfinite(s->proposal_sigma) || !std::isfinite(s->proposal_x0[0]) ||
+             !std::isfinite(s->proposal_x0[1]) || !std::isfinite(s->proposal_x0[2]))) {
+            return "proposal parameters must be finite";
+        }
     }
     if (n < 0 || (n > 0 && !probes)) return "null probes";
     return std::string();
@@ -136,6 +148,10 @@ int prepare_heat(wos_context *ctx, const wos_params *params, const wos_gaussian_
     h.x0[1] = src->x0[1];
     h.x0[2] = src->x0[2];
     h.sigma = src->sigma;
+    h.beta = src->mis_green_probability;
+    const bool own = !(src->proposal_sigma > 0.0);
+    for (int k = 0; k < 3; ++k) h.px0[k] = own ? src->x0[k] : src->proposal_x0[k];
+    h.psigma = own ? src->sigma : src->proposal_sigma;
     h.slot_verts = static_cast<const int *>(ctx->sdev.slotv.ptr);
     if (vertex_values) {
         const size_t nv = static_cast<size_t>(ctx->scene.n_verts);

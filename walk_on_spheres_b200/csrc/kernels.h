@@ -128,8 +128,10 @@ FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, in
 // Gaussian heat source -Δu = Q exp(-|x - x0|^2 / sigma^2) with per-vertex
 // Dirichlet data (kernels_adjoint.cu).
 struct HeatDesc {
-    int mode;               // kUniform / kGreen source sampling
+    int mode;               // kUniform / kGreen / kMis source sampling
     double Q, x0[3], sigma;
+    double beta;            // kMis: probability of a Green sample
+    double px0[3], psigma;  // kMis: proposal N(px0, psigma^2 / 2 I)
     const double *g;        // per-vertex boundary values (null: all zero)
     const int *slot_verts;  // per binary-tree slot: the primitive's dim vertex ids
     int adjoint;            // 0: forward walks; 1: replay accumulating derivatives

@@ -7,8 +7,10 @@
 // equation and no gradients; the estimator is its Poisson estimator
 // (include/wos/wos.hpp:54-138 with the Green kernels of
 // include/wos/poisson.hpp:12-51): every step adds green_mass(R) f(y) with y
-// Green-distributed in the ball (source mode green) or |B(R)| f(y) G(R, |y-x|)
-// with y uniform in the ball (uniform), then moves to a uniform point of the
+// Green-distributed in the ball (source mode green), |B(R)| f(y) G(R, |y-x|)
+// with y uniform in the ball (uniform), or the balance-heuristic mixture of
+// the Green density and a Gaussian proposal (MIS, include/wos/
+// source_sampling.hpp:35-78), then moves to a uniform point of the
 // sphere; inside the epsilon shell the walk ends with g at the nearest point.
 //
 // Derivatives.  A walk's geometry -- sphere centres, source samples y_k and
@@ -60,6 +62,8 @@ struct HeatArgs {
     int stage, stage_box, stage_prim;
     int mode;
     double Q, x0, y0, z0, inv_s2, inv_s;
+    double beta;                            // MIS: probability of a Green sample
+    double px0, py0, pz0, p_inv_s2, p_norm, p_scale;  // MIS proposal N(px0, psigma^2/2 I)
     const double *g;
     const int *slot_verts;
     int adjoint;
@@ -124,29 +128,72 @@ __device__ __forceinline__ double boundary_data(const HeatArgs &a, int slot, con
 }
 
 // Source term of one step from the ball B(p, R); adds its parameter
-// derivatives to j when `adj`.
-template <int DIM, typename T, class Rng>
-__device__ __forceinline__ double heat_source(const HeatArgs &a, V3<T> p, T R, Rng &rng,
+// derivatives to j when `adj`.  Every branch reduces to m * f(y) with a
+// weight m that does not depend on (Q, x0, sigma):
+//   Green    y ~ Green density of the ball,  m = green_mass(R)
+//   uniform  y ~ uniform in the ball,        m = |B(R)| G(R, |y - p|)
+//   MIS      y ~ beta Green + (1 - beta) proposal (include/wos/source_sampling.hpp:
+//            35-78), m = G / (beta G / green_mass + (1 - beta) p_proposal(y)),
+//            0 unless 0 < |y - p| < R; the proposal is a fixed density, so the
+//            derivatives are still m * df/dtheta.
+template <int DIM, typename T>
+__device__ __forceinline__ double heat_source(const HeatArgs &a, V3<T> p, T R, FastRng<T> &rng,
                                               bool adj, double j[5]) {
-    V3<T> y;
+    double yx, yy, yz;
     double m;
     const double Rd = static_cast<double>(R);
+    const double px = static_cast<double>(p.x), py = static_cast<double>(p.y);
+    const double pz = DIM == 3 ? static_cast<double>(p.z) : 0.0;
     if (a.mode == kGreen) {
         const T r = DIM == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
-        y = direction_at<DIM, false, T>(p, r, rng);
+        const V3<T> y = direction_at<DIM, false, T>(p, r, rng);
+        yx = static_cast<double>(y.x);
+        yy = static_cast<double>(y.y);
+        yz = DIM == 3 ? static_cast<double>(y.z) : 0.0;
         m = DIM == 2 ? Rd * Rd / 4.0 : Rd * Rd / 6.0;
+    } else if (a.mode == kMis) {
+        if (static_cast<double>(rng.unit()) < a.beta) {
+            const T r = DIM == 2 ? pg_sample_radius_2d(R, rng) : pg_sample_radius_3d(R, rng);
+            const V3<T> y = direction_at<DIM, false, T>(p, r, rng);
+            yx = static_cast<double>(y.x);
+            yy = static_cast<double>(y.y);
+            yz = DIM == 3 ? static_cast<double>(y.z) : 0.0;
+        } else {
+            // Box-Muller normals from FP64 uniforms
+            double s0, c0;
+            const double rho0 = sqrt(-2.0 * log(rng.s.uniform_d()));
+            sincospi(2.0 * rng.s.uniform_d(), &s0, &c0);
+            yx = a.px0 + a.p_scale * rho0 * c0;
+            yy = a.py0 + a.p_scale * rho0 * s0;
+            yz = 0.0;
+            if (DIM == 3) {
+                const double rho1 = sqrt(-2.0 * log(rng.s.uniform_d()));
+                yz = a.pz0 + a.p_scale * rho1 * cospi(2.0 * rng.s.uniform_d());
+            }
+        }
+        const double ex = yx - px, ey = yy - py, ez = yz - pz;
+        const double r = sqrt(ex * ex + ey * ey + ez * ez);
+        if (!(r > 0.0 && r < Rd)) return 0.0;
+        const double G = DIM == 2 ? pg_green_2d(Rd, r) : pg_green_3d(Rd, r);
+        const double mass = DIM == 2 ? Rd * Rd / 4.0 : Rd * Rd / 6.0;
+        const double qx = yx - a.px0, qy = yy - a.py0, qz = yz - a.pz0;
+        const double src_pdf = a.p_norm * exp(-(qx * qx + qy * qy + qz * qz) * a.p_inv_s2);
+        const double mix = a.beta * (G / mass) + (1.0 - a.beta) * src_pdf;
+        if (!(mix > 0.0)) return 0.0;
+        m = G / mix;
     } else {
-        y = ball_sample<DIM, false, T>(p, R, rng);
-        const double ex = static_cast<double>(y.x) - static_cast<double>(p.x);
-        const double ey = static_cast<double>(y.y) - static_cast<double>(p.y);
-        const double ez = DIM == 3 ? static_cast<double>(y.z) - static_cast<double>(p.z) : 0.0;
+        const V3<T> y = ball_sample<DIM, false, T>(p, R, rng);
+        yx = static_cast<double>(y.x);
+        yy = static_cast<double>(y.y);
+        yz = DIM == 3 ? static_cast<double>(y.z) : 0.0;
+        const double ex = yx - px, ey = yy - py, ez = yz - pz;
         const double r = fmin(sqrt(ex * ex + ey * ey + ez * ez), Rd);
         if (!(r > 0.0)) return 0.0;
         m = ball_volume<DIM, double>(Rd) * (DIM == 2 ? pg_green_2d(Rd, r) : pg_green_3d(Rd, r));
     }
-    const double dx = static_cast<double>(y.x) - a.x0;
-    const double dy = static_cast<double>(y.y) - a.y0;
-    const double dz = DIM == 3 ? static_cast<double>(y.z) - a.z0 : 0.0;
+    const double dx = yx - a.x0;
+    const double dy = yy - a.y0;
+    const double dz = DIM == 3 ? yz - a.z0 : 0.0;
     const double q = (dx * dx + dy * dy + dz * dz) * a.inv_s2;
     const double e = exp(-q);
     const double mf = m * a.Q * e;
@@ -532,6 +579,14 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
     a.z0 = s.dim == 3 ? h.x0[2] : 0.0;
     a.inv_s2 = 1.0 / (h.sigma * h.sigma);
     a.inv_s = 1.0 / h.sigma;
+    a.beta = h.beta;
+    a.px0 = h.px0[0];
+    a.py0 = h.px0[1];
+    a.pz0 = s.dim == 3 ? h.px0[2] : 0.0;
+    a.p_inv_s2 = 1.0 / (h.psigma * h.psigma);
+    // N(px0, psigma^2/2 I): density exp(-|y - px0|^2 / psigma^2) / (pi^(d/2) psigma^d)
+    a.p_norm = 1.0 / (std::pow(kPi, 0.5 * s.dim) * std::pow(h.psigma, s.dim));
+    a.p_scale = h.psigma / std::sqrt(2.0);
     a.g = h.g;
     a.slot_verts = h.slot_verts;
     a.adjoint = h.adjoint;

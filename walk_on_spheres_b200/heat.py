@@ -60,8 +60,15 @@ class HeatProblem:
 
     def __init__(self, solver: Solver, probes, N_walks: int = 2048, epsilon: float = 1e-5,
                  max_steps: int = 100000, max_ray_attempts: int = 12, seed: int = 0,
-                 source_mode="green", method="fast", point_index=None):
+                 source_mode="green", method="fast", point_index=None,
+                 mis_green_probability: float = 0.5, proposal=None):
+        """source_mode "uniform", "green" or "mis"; for "mis", each step takes a
+        Green sample with probability mis_green_probability, else a sample of the
+        proposal N(x0p, sigmap^2/2 I), proposal = (x0p, sigmap) held fixed across calls
+        (None: each call's own x0 and sigma)."""
         self.solver = solver
+        self.mis_green_probability = float(mis_green_probability)
+        self.proposal = proposal
         self.probes = np.ascontiguousarray(probes, dtype=np.float64).reshape(-1, solver.dim)
         self.n = self.probes.shape[0]
         self.point_index = (None if point_index is None
@@ -81,13 +88,17 @@ class HeatProblem:
         solver._check(solver._L.wos_mesh_vertex_count(solver._ctx, C.byref(nv)))
         self.n_verts = nv.value
 
-    @staticmethod
-    def _source(Q, x0, sigma) -> _lib.GaussianSource:
+    def _source(self, Q, x0, sigma) -> _lib.GaussianSource:
         s = _lib.GaussianSource()
         s.Q = float(Q)
         xs = [float(v) for v in np.asarray(x0, dtype=np.float64).ravel()] + [0.0, 0.0, 0.0]
         s.x0 = (C.c_double * 3)(*xs[:3])
         s.sigma = float(sigma)
+        s.mis_green_probability = self.mis_green_probability
+        if self.proposal is not None:
+            px = [float(v) for v in np.asarray(self.proposal[0], np.float64).ravel()] + [0.0] * 3
+            s.proposal_x0 = (C.c_double * 3)(*px[:3])
+            s.proposal_sigma = float(self.proposal[1])
         return s
 
     def _values(self, vertex_values):

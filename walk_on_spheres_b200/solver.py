@@ -24,7 +24,7 @@ from . import _lib
 
 EQUATIONS = ("laplace", "poisson", "screened_poisson", "helmholtz")
 METHODS = {"plain": 0, "fast": 1, "fast64": 2}
-SOURCE_MODES = {"uniform": 0, "green": 1}
+SOURCE_MODES = {"uniform": 0, "green": 1, "mis": 2}
 LOCATION_NAMES = {0: "Outside", 1: "Inside", 2: "Boundary", 3: "Indeterminate"}
 
 
