@@ -2,6 +2,7 @@
 
     python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0] [--tune]
     python -m walk_on_spheres_b200.benchmarks --batch [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks --heat [--scale 1.0]
 
 Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 
@@ -222,6 +223,49 @@ def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
     return out
 
 
+def run_heat(scale: float = 1.0, device: int = 0, seed: int = 7) -> dict:
+    """The differentiable heat-source workload: 3D Gaussian source Q = 1e3,
+    sigma = 2 mm, x0 at the centre of the top face of a 0.10 x 0.05 x 0.01 m
+    slab of ~20k triangles, g = 0, 4096 probes uniform in the interior,
+    2048 FP32 walks (times `scale`), epsilon 1e-5 m.  For Green and MIS source
+    sampling: forward and backward device times, walks and queries per
+    second, and the median relative standard error of the probe values and
+    of du/dQ over probes where the source is felt (|u| > 1e-6 max|u|)."""
+    from .heat import HeatProblem
+    slab = meshes.slab_box(target_triangles=20000)
+    s = Solver(device).set_mesh(slab)
+    rng = np.random.default_rng(20240)
+    hi = np.array([0.10, 0.05, 0.01])
+    probes = hi * rng.uniform(0.001, 0.999, size=(4096, 3))
+    walks = max(32, int(round(2048 * scale)))
+    theta = (1e3, (0.05, 0.025, 0.01), 2e-3)
+    out = {"workload": "heat3d_slab20k_4096probes", "walks": walks,
+           "triangles": int(slab.prims.shape[0]), "modes": {}}
+    for mode in ("green", "mis"):
+        heat = HeatProblem(s, probes, N_walks=walks, epsilon=1e-5, seed=seed, source_mode=mode,
+                           method="fast", proposal=(theta[1], theta[2]))
+        g = np.zeros(heat.n_verts)
+        heat.forward(*theta, g)
+        f = heat.forward(*theta, g)
+        a = heat.adjoint(*theta, g)
+        felt = np.abs(f.mean) > 1e-6 * np.nanmax(np.abs(f.mean))
+        rel = f.standard_error[felt] / np.abs(f.mean[felt])
+        jrel = a.jacobian_se[felt, 0] / np.abs(a.jacobian[felt, 0])
+        c, ca = f.counters, a.counters
+        out["modes"][mode] = {
+            "forward_ms": c["total_ms"], "backward_ms": ca["total_ms"],
+            "gradients_per_s": 1000.0 / ca["total_ms"],
+            "walks_per_s": c["total_walks"] / (c["walk_ms"] / 1000.0),
+            "queries_per_s": c["total_steps"] / (c["walk_ms"] / 1000.0),
+            "mean_steps": c["total_steps"] / max(1, c["total_walks"]),
+            "probes_felt": int(felt.sum()),
+            "median_rel_se_u": float(np.median(rel)),
+            "median_rel_se_dudQ": float(np.median(jrel)),
+            "grad_source": a.grad_source.tolist()}
+    s.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -232,7 +276,12 @@ def main(argv=None) -> int:
                     help="autotune the FAST_FP32 schedule and leaf size first")
     ap.add_argument("--batch", action="store_true",
                     help="run the 64-solve mixed batch instead of the single solves")
+    ap.add_argument("--heat", action="store_true",
+                    help="run the differentiable heat-source workload (Green and MIS)")
     a = ap.parse_args(argv)
+    if a.heat:
+        print(json.dumps(run_heat(a.scale, a.device)), flush=True)
+        return 0
     if a.batch:
         print(json.dumps(run_batch(a.scale, a.device)), flush=True)
         return 0

@@ -140,6 +140,46 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         }
         return WideResult{best, slot};
     }
+    // Heights 3 and 4: the same nearest-first order with one child bound per
+    // level held in a register, so going back up re-reads nothing.
+    if (w.H == 3) {
+        const float d2 = wide_box_dist<DIM>(w, 2, 0, px, py, pz);
+        unsigned m2 = __ballot_sync(kAll, d2 < limit);
+        while (m2) {
+            const int n2 = static_cast<int>(take_nearest(m2, d2));
+            const float d1 = wide_box_dist<DIM>(w, 1, n2, px, py, pz);
+            unsigned m1 = __ballot_sync(kAll, d1 < limit);
+            while (m1) {
+                const unsigned k = take_nearest(m1, d1);
+                leaf(n2 * 32 + static_cast<int>(k));
+                m1 &= __ballot_sync(kAll, d1 < limit);
+            }
+            m2 &= __ballot_sync(kAll, d2 < limit);
+        }
+        return WideResult{best, slot};
+    }
+    if (w.H == 4) {
+        const float d3 = wide_box_dist<DIM>(w, 3, 0, px, py, pz);
+        unsigned m3 = __ballot_sync(kAll, d3 < limit);
+        while (m3) {
+            const int n3 = static_cast<int>(take_nearest(m3, d3));
+            const float d2 = wide_box_dist<DIM>(w, 2, n3, px, py, pz);
+            unsigned m2 = __ballot_sync(kAll, d2 < limit);
+            while (m2) {
+                const int n2 = n3 * 32 + static_cast<int>(take_nearest(m2, d2));
+                const float d1 = wide_box_dist<DIM>(w, 1, n2, px, py, pz);
+                unsigned m1 = __ballot_sync(kAll, d1 < limit);
+                while (m1) {
+                    const unsigned k = take_nearest(m1, d1);
+                    leaf(n2 * 32 + static_cast<int>(k));
+                    m1 &= __ballot_sync(kAll, d1 < limit);
+                }
+                m2 &= __ballot_sync(kAll, d2 < limit);
+            }
+            m3 &= __ballot_sync(kAll, d3 < limit);
+        }
+        return WideResult{best, slot};
+    }
     int h = w.H;    // height of the current node
     int node = 0;   // its index at that height
     float d = wide_box_dist<DIM>(w, h - 1, node, px, py, pz);

@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
     constexpr bool kF32 = std::is_same<T, float>::value;
     extern __shared__ float4 smem[];
     __shared__ int s_off[8];
+    __shared__ double s_acc[10][256];
     if (threadIdx.x < 8) s_off[threadIdx.x] = a.w.off[threadIdx.x];
     WideView wv = a.w;
     wv.off = s_off;
@@ -255,7 +256,12 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
 
         int n_acc = 0, steps_acc = 0;
         double mean_acc = 0.0, m2_acc = 0.0;
-        double jsum[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, jsq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        // per-lane sums and sums of squares of the derivatives, in shared
+        // memory (touched once per finished walk) to keep registers for the walk
+        if (adj) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) s_acc[k][threadIdx.x] = 0.0;
+        }
         unsigned hits = 0;
 
         int walk = w0 + lane;
@@ -365,8 +371,8 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                 if (adj) {
 #pragma unroll
                     for (int k = 0; k < 5; ++k) {
-                        jsum[k] += j[k];
-                        jsq[k] += j[k] * j[k];
+                        s_acc[k][threadIdx.x] += j[k];
+                        s_acc[5 + k][threadIdx.x] += j[k] * j[k];
                     }
                 }
             }
@@ -402,7 +408,13 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             steps_tot += sb;
             hits += hb;
         }
+        double jsum[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, jsq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         if (adj) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                jsum[k] = s_acc[k][threadIdx.x];
+                jsq[k] = s_acc[5 + k][threadIdx.x];
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -525,8 +537,10 @@ cudaError_t launch_heat_dim(const HeatArgs &a, int precision, const FastPlan &pl
     };
     int blocks = 0;
     if (precision == 32) {
-        auto k = heat_walk_kernel<DIM, float, 2>;
-        if (plan.smem_bytes > 48 * 1024) {
+        auto k = heat_walk_kernel<DIM, float, 3>;
+        // the static accumulators (20 KB) plus the staged scene can pass the
+        // 48 KB default: opt in whenever anything is staged
+        if (plan.smem_bytes > 0) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  plan.smem_bytes);
             if (e != cudaSuccess) return e;
