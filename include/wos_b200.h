@@ -238,6 +238,49 @@ int wos_batch_result(wos_batch *batch, int solve_id, double *mean, double *varia
                      double *standard_error, double *mean_steps, uint8_t *location,
                      wos_counters *counters);
 
+/* ------------------------------------------------- transient plate heating */
+
+/* The reference's transient welding baseline (apps/welding/src/
+ * level2_transient_heat.cpp, Level2Config:46-78): a rectangular plate
+ * length_x x length_y centred on the origin, zero temperature rise on its
+ * edges, a stationary Gaussian heat source normalised on the finite plate
+ * (apps/welding/include/welding/gaussian_heat_source.hpp) switched on for
+ * heat_on_time, implicit Euler steps of dt up to total_time, each solved by
+ * screened walk on spheres with alpha = 1/sqrt(kappa dt) and the source
+ * alpha^2 max(0, u_prev) + fraction q/k, u_prev sampled from the previous
+ * step's grid field (bilinear or cubic, FieldSampler2D).  Seeds per step and
+ * point as the reference: splitmix64(seed ^ splitmix64(step) ^
+ * splitmix64(i*ny + j)); PLAIN_FP64 follows the reference's streams. */
+typedef struct {
+    int nx, ny;                /* odd, >= 3 */
+    double dt, total_time, heat_on_time;
+    int walks, max_steps;
+    double epsilon;
+    uint64_t seed;
+    int cubic;                 /* history interpolation: 1 cubic, 0 bilinear */
+    double length_x, length_y, thickness;
+    double conductivity, density, specific_heat;
+    double electrical_power, efficiency, sigma_x, sigma_y;
+    int method;                /* WOS_METHOD_* */
+} wos_transient_params;
+
+/* The reference's defaults (Level2Config:46-78). */
+void wos_transient_defaults(wos_transient_params *p);
+
+/* Number of time steps of p (total_time / dt), or -1 if p is invalid. */
+int wos_transient_steps(const wos_transient_params *p);
+
+/* Run every time step on the context's device (the context's mesh is not
+ * used or changed).  fields / standard_error (host, may be NULL):
+ * (steps + 1) x nx x ny doubles, step 0 the zero initial field.
+ * max_steps_hits (may be NULL): summed over all steps.  use_graph != 0
+ * captures the whole time loop as one CUDA graph before launching it.
+ * device_ms (may be NULL): device time of all steps.  Parameter errors
+ * carry the reference's messages (level2_transient_heat.cpp:206-223). */
+int wos_transient_solve(wos_context *ctx, const wos_transient_params *p, int use_graph,
+                        double *fields, double *standard_error, long long *max_steps_hits,
+                        float *device_ms);
+
 /* ------------------------------------ Gaussian heat source and its adjoint */
 
 /* Source of the differentiable heat problem (no reference counterpart; the

@@ -59,6 +59,19 @@ class GaussianSource(C.Structure):
                 ("proposal_sigma", C.c_double)]
 
 
+class TransientParams(C.Structure):
+    """wos_transient_params (the reference's Level2Config plus the walk method)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dt", C.c_double),
+                ("total_time", C.c_double), ("heat_on_time", C.c_double),
+                ("walks", C.c_int), ("max_steps", C.c_int), ("epsilon", C.c_double),
+                ("seed", C.c_uint64), ("cubic", C.c_int), ("length_x", C.c_double),
+                ("length_y", C.c_double), ("thickness", C.c_double),
+                ("conductivity", C.c_double), ("density", C.c_double),
+                ("specific_heat", C.c_double), ("electrical_power", C.c_double),
+                ("efficiency", C.c_double), ("sigma_x", C.c_double), ("sigma_y", C.c_double),
+                ("method", C.c_int)]
+
+
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
                      C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double,
                      C.c_int)
@@ -91,6 +104,10 @@ SIGNATURES = {
     "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
     "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
+    "wos_transient_defaults": (None, [C.POINTER(TransientParams)]),
+    "wos_transient_steps": (C.c_int, [C.POINTER(TransientParams)]),
+    "wos_transient_solve": (C.c_int, [VP, C.POINTER(TransientParams), C.c_int, VP, VP,
+                                      C.POINTER(C.c_longlong), C.POINTER(C.c_float)]),
     "wos_batch_create": (C.c_int, [VP, C.POINTER(VP)]),
     "wos_batch_destroy": (None, [VP]),
     "wos_batch_add_mesh": (C.c_int, [VP, C.c_int, VP, C.c_int, VP, C.c_int, VP, C.c_int,

@@ -44,6 +44,7 @@ CUDA_UNITS = {
     "context.cpp": ["-x", "cu"],
     "heat_api.cpp": ["-x", "cu"],
     "batch.cpp": ["-x", "cu"],
+    "transient.cpp": ["-x", "cu"],
     "noalloc.cu": [],
 }
 HOST_UNITS = ["scene_build.cpp", "obj_reader.cpp", "runner.cpp", "h5_writer.cpp", "host_api.cpp"]

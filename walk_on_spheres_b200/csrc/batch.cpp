@@ -183,7 +183,7 @@ int wos_batch::plan() {
                               effective_epsilon(b.p), b.p.max_steps,
                               std::ldexp(m.scene.scale, -16), pl, loc + b.point_begin,
                               st + b.point_begin, part + b.task_off, nullptr, ctr + order[i]);
-        it.eq = EqDesc{b.p.equation, b.p.source_mode, b.p.alpha};
+        it.eq = EqDesc{b.p.equation, b.p.source_mode, b.p.alpha, nullptr};
         it.out = Fields{static_cast<double *>(f_mean.ptr) + b.point_begin,
                         static_cast<double *>(f_var.ptr) + b.point_begin,
                         static_cast<double *>(f_se.ptr) + b.point_begin,

@@ -287,7 +287,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     WOS_CUDA(this, cudaMemsetAsync(counters.ptr, 0, sizeof(DeviceCounters), stream),
              "clear counters");
 
-    EqDesc eq{p.equation, p.source_mode, p.alpha};
+    EqDesc eq{p.equation, p.source_mode, p.alpha, nullptr};
     const double eps = effective_epsilon(p);
     // boundary tolerance 1e-10 * max(1, mesh extents), include/wos/runner.hpp:86-88
     const double btol = 1e-10 * scene.scale;

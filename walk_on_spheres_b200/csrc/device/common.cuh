@@ -57,9 +57,10 @@ struct StartRecord {
 
 // Equation selection for runtime dispatch.
 struct EqDesc {
-    int kind;    // kLaplace ... kHelmholtz
+    int kind;    // kLaplace ... kHelmholtz, kTransient (2D only)
     int mode;    // kUniform / kGreen
     double alpha;
+    const TransientDesc *tr;  // kTransient: the step's descriptor (device memory)
 };
 
 // Per-solve device counters (include/wos/runner.hpp:147-151).
@@ -92,6 +93,7 @@ __device__ __forceinline__ double boundary_value(const EqDesc &e, V3<double> p, 
         case kLaplace: return Laplace<DIM>{}.boundary(p, bid);
         case kPoisson: return Poisson<DIM>{e.mode, e.alpha}.boundary(p, bid);
         case kScreened: return Screened<DIM>{e.mode, e.alpha}.boundary(p, bid);
+        case kTransient: return 0.0;
         default: return Helmholtz<DIM>{}.boundary(p, bid);
     }
 }

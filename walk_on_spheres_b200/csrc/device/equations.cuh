@@ -19,7 +19,7 @@
 
 namespace wosb {
 
-enum : int { kLaplace = 0, kPoisson = 1, kScreened = 2, kHelmholtz = 3 };
+enum : int { kLaplace = 0, kPoisson = 1, kScreened = 2, kHelmholtz = 3, kTransient = 4 };
 enum : int { kUniform = 0, kGreen = 1, kMis = 2 };
 
 template <typename T>
@@ -431,6 +431,123 @@ struct Helmholtz {
         if (prod < T(1e-8)) return T(1);
         return DIM == 2 ? T(1) / bessel_j0(prod) : prod / sin(prod);
     }
+};
+
+// One implicit-Euler step of the transient plate heat problem
+// (apps/welding/src/level2_transient_heat.cpp:237-292): screened Poisson with
+// alpha = 1/sqrt(kappa dt), zero boundary data and the source
+//   alpha^2 max(0, u_prev(x)) + fraction * q_v(x) / k,
+// u_prev read from the previous step's grid field by the reference's
+// FieldSampler2D (apps/welding/include/welding/field_sampler.hpp:32-126) and
+// q_v the finite-plate Gaussian power density of
+// apps/welding/include/welding/gaussian_heat_source.hpp:38-41, 112-123.
+// Expression order follows the reference (the exact path rounds like it).
+struct TransientDesc {
+    double alpha;
+    double fraction;       // share of the step with the heat source on
+    double conductivity;
+    double power;          // absorbed power
+    double thickness, ix, iy;  // plate thickness, Gaussian integrals over x and y
+    double cx, cy, sx, sy;
+    const double *prev;    // previous field, (i, j) row-major, nx * ny
+    int nx, ny;
+    double xmin, xmax, ymin, ymax;
+    int cubic;             // 1: cubic Lagrange history interpolation, 0: bilinear
+    int pad;
+};
+
+__device__ __forceinline__ double clamp_ref(double v, double lo, double hi) {
+    return v < lo ? lo : (hi < v ? hi : v);  // std::clamp
+}
+
+__device__ __forceinline__ double field_at(const TransientDesc &t, int i, int j) {
+    return t.prev[static_cast<long long>(i) * t.ny + j];
+}
+
+__device__ __forceinline__ void cubic_weights(double c, double w[4]) {
+    w[0] = -(c - 1.0) * (c - 2.0) * (c - 3.0) / 6.0;
+    w[1] = c * (c - 2.0) * (c - 3.0) / 2.0;
+    w[2] = -c * (c - 1.0) * (c - 3.0) / 2.0;
+    w[3] = c * (c - 1.0) * (c - 2.0) / 6.0;
+}
+
+// FieldSampler2D::sample
+__device__ __forceinline__ double field_sample(const TransientDesc &t, double x, double y) {
+    const double gx = clamp_ref((x - t.xmin) / (t.xmax - t.xmin) * static_cast<double>(t.nx - 1),
+                                0.0, static_cast<double>(t.nx - 1));
+    const double gy = clamp_ref((y - t.ymin) / (t.ymax - t.ymin) * static_cast<double>(t.ny - 1),
+                                0.0, static_cast<double>(t.ny - 1));
+    if (t.cubic && t.nx >= 4 && t.ny >= 4) {
+        int ix = static_cast<int>(floor(gx)) - 1;
+        int iy = static_cast<int>(floor(gy)) - 1;
+        ix = ix < 0 ? 0 : (t.nx - 4 < ix ? t.nx - 4 : ix);
+        iy = iy < 0 ? 0 : (t.ny - 4 < iy ? t.ny - 4 : iy);
+        double wx[4], wy[4];
+        cubic_weights(gx - static_cast<double>(ix), wx);
+        cubic_weights(gy - static_cast<double>(iy), wy);
+        double value = 0.0;
+        for (int di = 0; di < 4; ++di) {
+            double row = 0.0;
+            for (int dj = 0; dj < 4; ++dj) row += wy[dj] * field_at(t, ix + di, iy + dj);
+            value += wx[di] * row;
+        }
+        return value;
+    }
+    const int i0 = static_cast<int>(floor(gx));
+    const int j0 = static_cast<int>(floor(gy));
+    const int i1 = i0 + 1 < t.nx - 1 ? i0 + 1 : t.nx - 1;
+    const int j1 = j0 + 1 < t.ny - 1 ? j0 + 1 : t.ny - 1;
+    const double tx = gx - static_cast<double>(i0);
+    const double ty = gy - static_cast<double>(j0);
+    const double v00 = field_at(t, i0, j0);
+    const double v10 = field_at(t, i1, j0);
+    const double v01 = field_at(t, i0, j1);
+    const double v11 = field_at(t, i1, j1);
+    const double lower = (1.0 - tx) * v00 + tx * v10;
+    const double upper = (1.0 - tx) * v01 + tx * v11;
+    return (1.0 - ty) * lower + ty * upper;
+}
+
+// TransientGaussianHeat2D::source
+__device__ __forceinline__ double transient_source(const TransientDesc &t, double x, double y) {
+    const double v = field_sample(t, x, y);
+    const double previous = t.alpha * t.alpha * (0.0 < v ? v : 0.0);
+    double heat = 0.0;
+    if (t.fraction > 0.0) {
+        const double dx = (x - t.cx) / t.sx;
+        const double dy = (y - t.cy) / t.sy;
+        const double shape = exp(-0.5 * (dx * dx + dy * dy));
+        const double density = t.power * shape / (t.thickness * t.ix * t.iy);
+        heat = t.fraction * density / t.conductivity;
+    }
+    return previous + heat;
+}
+
+template <int DIM>
+struct Transient {
+    static constexpr bool kSource = true, kScreening = true;
+    int mode;  // always kGreen: screened Green source samples
+    double alpha;
+    const TransientDesc *t;
+    template <typename T>
+    __device__ T boundary(V3<T>, int) const { return T(0); }
+    template <typename T>
+    __device__ bool may_intersect(V3<T>, T) const { return true; }
+    template <typename T>
+    __device__ T source(V3<T> p) const {
+        return static_cast<T>(transient_source(*t, static_cast<double>(p.x),
+                                               static_cast<double>(p.y)));
+    }
+    template <typename T>
+    __device__ T green(T R, T r) const { return sc_green_2d(static_cast<T>(alpha), R, r); }
+    template <typename T>
+    __device__ T green_mass(T R) const { return sc_mass_2d(static_cast<T>(alpha), R); }
+    template <typename T, class Rng>
+    __device__ T green_radius(T R, Rng &rng, bool &overflow) const {
+        return sc_sample_radius_2d(static_cast<T>(alpha), R, rng, overflow);
+    }
+    template <typename T>
+    __device__ T screening(T R) const { return sc_weight_2d(static_cast<T>(alpha), R); }
 };
 
 // One iteration of the walk loop body before the closest-point query

@@ -29,7 +29,7 @@ int wos_context::run_heat(const wos_params &p, const HeatDesc &h, const PointSet
     // boundary tolerance 1e-10 * max(1, mesh extents), include/wos/runner.hpp:86-88
     const double btol = 1e-10 * scene.scale;
     // classification only: the heat merge writes every field
-    const EqDesc eq{kLaplace, 0, 0.0};
+    const EqDesc eq{kLaplace, 0, 0.0, nullptr};
     const Fields cls{nullptr, nullptr, nullptr, nullptr, out.f.location};
 
     WOS_CUDA(this, cudaEventRecord(events[0], stream), "event");

@@ -248,6 +248,12 @@ void launch_plain_dim(const SceneView &s, const PointSet &ps, uint64_t seed, EqD
             launch_plain_typed<DIM>(s, ps, seed, Screened<DIM>{e.mode, e.alpha}, n_walks, eps,
                                     max_steps, location, start, out, ctr, stream);
             break;
+        case kTransient:
+            if (DIM == 2) {
+                launch_plain_typed<2>(s, ps, seed, Transient<2>{kGreen, e.alpha, e.tr}, n_walks,
+                                      eps, max_steps, location, start, out, ctr, stream);
+            }
+            break;
         default:
             launch_plain_typed<DIM>(s, ps, seed, Helmholtz<DIM>{}, n_walks, eps, max_steps,
                                     location, start, out, ctr, stream);

@@ -468,6 +468,8 @@ Screened<3> eq_host(const EqDesc &e) { return Screened<3>{e.mode, e.alpha}; }
 template <>
 Helmholtz<2> eq_host(const EqDesc &) { return Helmholtz<2>{}; }
 template <>
+Transient<2> eq_host(const EqDesc &e) { return Transient<2>{kGreen, e.alpha, e.tr}; }
+template <>
 Helmholtz<3> eq_host(const EqDesc &) { return Helmholtz<3>{}; }
 
 template <int DIM, class Eq>
@@ -521,6 +523,9 @@ cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const Fa
             return launch_fast_typed<DIM, Poisson<DIM>>(a, e, precision, plan, stream);
         case kScreened:
             return launch_fast_typed<DIM, Screened<DIM>>(a, e, precision, plan, stream);
+        case kTransient:
+            return DIM == 2 ? launch_fast_typed<2, Transient<2>>(a, e, precision, plan, stream)
+                            : cudaErrorInvalidValue;
         default:
             return launch_fast_typed<DIM, Helmholtz<DIM>>(a, e, precision, plan, stream);
     }
