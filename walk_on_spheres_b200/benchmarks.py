@@ -3,6 +3,7 @@
     python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0] [--tune]
     python -m walk_on_spheres_b200.benchmarks --batch [--scale 1.0]
     python -m walk_on_spheres_b200.benchmarks --heat [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks --transient [--scale 1.0]
 
 Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 
@@ -266,6 +267,30 @@ def run_heat(scale: float = 1.0, device: int = 0, seed: int = 7) -> dict:
     return out
 
 
+def run_transient(scale: float = 1.0, device: int = 0) -> dict:
+    """The reference's level-2 transient welding baseline at its defaults
+    (49 x 33 grid, 100 steps of 0.1 s, 500 walks, epsilon 8e-6 m; walks
+    times `scale`), one CUDA graph per run, for each walk method."""
+    from .transient import solve_transient
+    s = Solver(device)
+    walks = max(8, int(round(500 * scale)))
+    out = {"workload": "level2_plate_49x33_100steps", "walks": walks, "methods": {}}
+    for method in ("fast", "fast64", "plain"):
+        solve_transient(s, method=method, walks=walks, total_time=0.2, heat_on_time=0.1)  # warm-up
+        r = solve_transient(s, method=method, walks=walks)
+        inner = r.fields[:, 1:-1, 1:-1]
+        n_walks = (r.fields.shape[1] - 2) * (r.fields.shape[2] - 2) * walks * r.steps
+        out["methods"][method] = {
+            "device_ms": r.device_ms, "walks_per_s": n_walks / (r.device_ms / 1000.0),
+            "centre_rise_final": float(r.fields[-1, r.fields.shape[1] // 2,
+                                                r.fields.shape[2] // 2]),
+            "peak_rise": float(inner.max()),
+            "mean_se_final": float(r.standard_error[-1, 1:-1, 1:-1].mean()),
+            "max_steps_hits": r.max_steps_hits}
+    s.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -278,7 +303,12 @@ def main(argv=None) -> int:
                     help="run the 64-solve mixed batch instead of the single solves")
     ap.add_argument("--heat", action="store_true",
                     help="run the differentiable heat-source workload (Green and MIS)")
+    ap.add_argument("--transient", action="store_true",
+                    help="run the transient plate heating workload (reference level 2)")
     a = ap.parse_args(argv)
+    if a.transient:
+        print(json.dumps(run_transient(a.scale, a.device)), flush=True)
+        return 0
     if a.heat:
         print(json.dumps(run_heat(a.scale, a.device)), flush=True)
         return 0
