@@ -240,17 +240,26 @@ int wos_batch_result(wos_batch *batch, int solve_id, double *mean, double *varia
 
 /* ------------------------------------------------- transient plate heating */
 
-/* The reference's transient welding baseline (apps/welding/src/
- * level2_transient_heat.cpp, Level2Config:46-78): a rectangular plate
- * length_x x length_y centred on the origin, zero temperature rise on its
- * edges, a stationary Gaussian heat source normalised on the finite plate
- * (apps/welding/include/welding/gaussian_heat_source.hpp) switched on for
- * heat_on_time, implicit Euler steps of dt up to total_time, each solved by
- * screened walk on spheres with alpha = 1/sqrt(kappa dt) and the source
- * alpha^2 max(0, u_prev) + fraction q/k, u_prev sampled from the previous
- * step's grid field (bilinear or cubic, FieldSampler2D).  Seeds per step and
- * point as the reference: splitmix64(seed ^ splitmix64(step) ^
- * splitmix64(i*ny + j)); PLAIN_FP64 follows the reference's streams. */
+/* The reference's transient welding programs (apps/welding/src/
+ * level{0_cooling,2_transient_heat,3_moving_heat}.cpp): a rectangular plate
+ * [plate_x0, plate_x0 + length_x] x [plate_y0, plate_y0 + length_y] with zero
+ * temperature rise on its edges and implicit Euler steps of dt up to
+ * total_time, each solved by screened walk on spheres with
+ * alpha = 1/sqrt(kappa dt), kappa = conductivity / (density specific_heat),
+ * and a source built from the previous step's grid field u_prev (sampled
+ * bilinearly or by cubic Lagrange weights, FieldSampler2D):
+ *   scenario 0  alpha^2 u_prev                          (level 0, cooling)
+ *   scenario 2  alpha^2 max(0, u_prev) + f q/k, a stationary Gaussian at the
+ *               plate centre normalised on the finite plate
+ *               (gaussian_heat_source.hpp), f the share of the step before
+ *               heat_on_time                           (level 2)
+ *   scenario 3  alpha^2 max(0, u_prev) + q/k, a Gaussian moving along
+ *               y = weld_y from source_start_x at weld_speed until
+ *               heat_on_time, two Gauss-Legendre components per step
+ *               (moving_gaussian_heat_source.hpp)      (level 3)
+ * Seeds per step and point as the reference: splitmix64(seed ^
+ * splitmix64(step) ^ splitmix64(i*ny + j)); PLAIN_FP64 follows the
+ * reference's streams. */
 typedef struct {
     int nx, ny;                /* odd, >= 3 */
     double dt, total_time, heat_on_time;
@@ -262,24 +271,29 @@ typedef struct {
     double conductivity, density, specific_heat;
     double electrical_power, efficiency, sigma_x, sigma_y;
     int method;                /* WOS_METHOD_* */
+    int scenario;              /* 0, 2 or 3 (above) */
+    double plate_x0, plate_y0; /* lower-left corner of the plate */
+    double weld_y, source_start_x, weld_speed;  /* scenario 3 */
 } wos_transient_params;
 
-/* The reference's defaults (Level2Config:46-78). */
+/* The reference's level-2 defaults (Level2Config:46-78), scenario 2. */
 void wos_transient_defaults(wos_transient_params *p);
 
 /* Number of time steps of p (total_time / dt), or -1 if p is invalid. */
 int wos_transient_steps(const wos_transient_params *p);
 
 /* Run every time step on the context's device (the context's mesh is not
- * used or changed).  fields / standard_error (host, may be NULL):
- * (steps + 1) x nx x ny doubles, step 0 the zero initial field.
- * max_steps_hits (may be NULL): summed over all steps.  use_graph != 0
- * captures the whole time loop as one CUDA graph before launching it.
- * device_ms (may be NULL): device time of all steps.  Parameter errors
- * carry the reference's messages (level2_transient_heat.cpp:206-223). */
-int wos_transient_solve(wos_context *ctx, const wos_transient_params *p, int use_graph,
-                        double *fields, double *standard_error, long long *max_steps_hits,
-                        float *device_ms);
+ * used or changed).  initial (host, may be NULL for zeros): the nx x ny
+ * field at time 0.  fields / standard_error (host, may be NULL):
+ * (steps + 1) x nx x ny doubles, step 0 the initial field.  max_steps_hits
+ * (may be NULL): summed over all steps.  use_graph != 0 captures the whole
+ * time loop as one CUDA graph before launching it.  device_ms (may be NULL):
+ * device time of all steps.  Parameter errors carry the reference's
+ * messages (level2_transient_heat.cpp:206-223, moving_gaussian_heat_source.hpp:
+ * 21-28, 55-58). */
+int wos_transient_solve(wos_context *ctx, const wos_transient_params *p, const double *initial,
+                        int use_graph, double *fields, double *standard_error,
+                        long long *max_steps_hits, float *device_ms);
 
 /* ------------------------------------ Gaussian heat source and its adjoint */
 

@@ -1,13 +1,15 @@
 """Transient plate heating (wos_transient_solve) against the reference's own
-level-2 program (tests/golden/level2_golden.npz, written by
-tests/golden/make_level2_golden.py from oracle/_ref/wos_level2_ref).
+welding programs -- level 0 (cooling), level 2 (stationary source) and
+level 3 (moving source) -- through tests/golden/transient_golden.npz, written
+by tests/golden/make_transient_golden.py from oracle/_ref/wos_level*_ref.
 
 Tolerances:
 * PLAIN_FP64 follows the reference's seeds and streams step by step: at
-  every step at least 98% of interior points agree with the reference to
-  1e-9 relative and every point within 4 of the reference's standard errors
-  (the same rule as the single-solve parity tests; CUDA's and glibc's
-  transcendental functions differ in the last bit).
+  every stored step at least 98% of interior points agree with the
+  reference to 1e-9 relative (level 0 prints six significant digits: 1e-5)
+  and every point within 4 of the reference's standard errors (the rule of
+  the single-solve parity tests; CUDA's and glibc's transcendental functions
+  differ in the last bit).
 * FAST_FP32 (other streams) against PLAIN_FP64 at step 1 (no history yet):
   >= 99% of interior points within 4.5 combined standard errors.  Later
   steps also carry the noise of the sampled history field, which the
@@ -18,6 +20,7 @@ Tolerances:
 from __future__ import annotations
 
 import json
+import math
 from pathlib import Path
 
 import numpy as np
@@ -25,37 +28,56 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = Path(__file__).resolve().parent / "golden" / "level2_golden.npz"
+GOLDEN = Path(__file__).resolve().parent / "golden" / "transient_golden.npz"
 
 
 def _cases():
     g = np.load(GOLDEN)
-    return [(k[:-len("_config")], json.loads(str(g[k]))) for k in g.files
+    return [(k[:-len("_config")], json.loads(str(g[k]))) for k in sorted(g.files)
             if k.endswith("_config")]
 
 
-@pytest.mark.parametrize("name,opts", _cases(), ids=[c[0] for c in _cases()])
-def test_plain_matches_reference_program(solver, name, opts):
+def params_for(cfg: dict) -> tuple[dict, np.ndarray | None]:
+    """Library parameters (and initial field) of a reference program's options."""
+    from walk_on_spheres_b200.transient import LEVEL0, LEVEL3
+    level = cfg["level"]
+    if level == 2:
+        keys = ("nx", "ny", "dt", "total_time", "heat_on_time", "walks", "seed", "cubic")
+        return {k: cfg[k] for k in keys}, None
+    if level == 3:
+        return dict(LEVEL3, walks=cfg["walks"], seed=cfg["seed"]), None
+    n = cfg["grid"]
+    p = dict(LEVEL0, nx=n, ny=n, dt=cfg["dt"], total_time=cfg["steps"] * cfg["dt"],
+             walks=cfg["walks"], epsilon=cfg["epsilon"], seed=cfg["seed"],
+             conductivity=cfg["diffusivity"])
+    # sin(pi x) sin(pi y) with the C library's sin, as the reference computes it
+    init = np.zeros((n, n))
+    for i in range(1, n - 1):
+        for j in range(1, n - 1):
+            init[i, j] = math.sin(math.pi * (i / (n - 1))) * math.sin(math.pi * (j / (n - 1)))
+    return p, init
+
+
+@pytest.mark.parametrize("name,cfg", _cases(), ids=[c[0] for c in _cases()])
+def test_plain_matches_reference_program(solver, name, cfg):
     from walk_on_spheres_b200.transient import solve_transient
     g = np.load(GOLDEN)
-    ref, ref_se = g[f"{name}_rise"], g[f"{name}_se"]
-    r = solve_transient(solver, method="plain", use_graph=False, **opts)
-    assert r.fields.shape == ref.shape
-    assert np.all(r.fields[0] == 0.0)
+    steps, ref, ref_se = g[f"{name}_steps"], g[f"{name}_rise"], g[f"{name}_se"]
+    params, init = params_for(cfg)
+    r = solve_transient(solver, method="plain", use_graph=True, initial=init, **params)
+    assert r.fields.shape[1:] == ref.shape[1:]
+    rtol = 1e-5 if cfg["level"] == 0 else 1e-9
     interior = np.zeros(ref.shape[1:], dtype=bool)
     interior[1:-1, 1:-1] = True
-    for s in range(ref.shape[0]):
+    for k, s in enumerate(steps):
         assert np.all(r.fields[s][~interior] == 0.0)
-        got, want = r.fields[s][interior], ref[s][interior]
-        close = np.abs(got - want) <= 1e-9 * np.maximum(1.0, np.abs(want))
+        got, want = r.fields[s][interior], ref[k][interior]
+        close = np.abs(got - want) <= rtol * np.maximum(1e-3, np.abs(want))
         assert close.mean() >= 0.98, (s, close.mean())
         far = ~close
         if far.any():
-            z = np.abs(got[far] - want[far]) / np.maximum(ref_se[s][interior][far], 1e-300)
+            z = np.abs(got[far] - want[far]) / np.maximum(ref_se[k][interior][far], 1e-300)
             assert (z <= 4.0).all(), (s, z.max())
-        se_close = np.abs(r.standard_error[s][interior] - ref_se[s][interior]) <= \
-            1e-9 * np.maximum(1.0, ref_se[s][interior])
-        assert se_close.mean() >= 0.98
 
 
 @pytest.mark.parametrize("method", ["fast", "fast64"])

@@ -11,7 +11,7 @@ import numpy as np
 from walk_on_spheres_b200 import _lib
 from walk_on_spheres_b200.transient import defaults, make_params
 
-GOLDEN = Path(__file__).resolve().parent / "golden" / "level2_golden.npz"
+GOLDEN = Path(__file__).resolve().parent / "golden" / "transient_golden.npz"
 
 
 def test_defaults_are_the_reference_level2_config():
@@ -43,13 +43,24 @@ def test_golden_fields_layout():
     for k in g.files:
         if not k.endswith("_config"):
             continue
-        name, opts = k[:-len("_config")], json.loads(str(g[k]))
-        rise = g[f"{name}_rise"]
-        steps = int(round(opts["total_time"] / opts["dt"]))
-        assert rise.shape == (steps + 1, opts["nx"], opts["ny"])
-        assert np.all(rise[0] == 0.0)
+        name, cfg = k[:-len("_config")], json.loads(str(g[k]))
+        rise, steps = g[f"{name}_rise"], g[f"{name}_steps"]
+        assert rise.shape[0] == steps.shape[0] and steps[0] == 0
         # zero temperature rise on the plate edges at every step
         assert np.all(rise[:, 0, :] == 0.0) and np.all(rise[:, -1, :] == 0.0)
         assert np.all(rise[:, :, 0] == 0.0) and np.all(rise[:, :, -1] == 0.0)
-        # heating makes the centre warm
-        assert rise[-1, opts["nx"] // 2, opts["ny"] // 2] > 0.0
+        c = (rise.shape[1] // 2, rise.shape[2] // 2)
+        if cfg["level"] == 0:
+            # cooling: the centre starts at sin(pi/2)^2 = 1 and decays
+            assert abs(rise[0][c] - 1.0) < 1e-6 and rise[-1][c] < rise[0][c]
+        else:
+            assert np.all(rise[0] == 0.0) and rise[-1][c] > 0.0
+
+
+def test_level_presets_are_valid():
+    from walk_on_spheres_b200.transient import LEVEL0, LEVEL3, level0_initial
+    L = _lib.lib()
+    assert L.wos_transient_steps(C.byref(make_params(**LEVEL0))) == 5
+    assert L.wos_transient_steps(C.byref(make_params(**LEVEL3))) == 150
+    f = level0_initial()
+    assert f.shape == (17, 17) and abs(f[8, 8] - 1.0) < 1e-15 and f[0].max() == 0.0

@@ -69,7 +69,9 @@ class TransientParams(C.Structure):
                 ("conductivity", C.c_double), ("density", C.c_double),
                 ("specific_heat", C.c_double), ("electrical_power", C.c_double),
                 ("efficiency", C.c_double), ("sigma_x", C.c_double), ("sigma_y", C.c_double),
-                ("method", C.c_int)]
+                ("method", C.c_int), ("scenario", C.c_int), ("plate_x0", C.c_double),
+                ("plate_y0", C.c_double), ("weld_y", C.c_double), ("source_start_x", C.c_double),
+                ("weld_speed", C.c_double)]
 
 
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
@@ -106,7 +108,7 @@ SIGNATURES = {
     "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
     "wos_transient_defaults": (None, [C.POINTER(TransientParams)]),
     "wos_transient_steps": (C.c_int, [C.POINTER(TransientParams)]),
-    "wos_transient_solve": (C.c_int, [VP, C.POINTER(TransientParams), C.c_int, VP, VP,
+    "wos_transient_solve": (C.c_int, [VP, C.POINTER(TransientParams), VP, C.c_int, VP, VP,
                                       C.POINTER(C.c_longlong), C.POINTER(C.c_float)]),
     "wos_batch_create": (C.c_int, [VP, C.POINTER(VP)]),
     "wos_batch_destroy": (None, [VP]),

@@ -433,22 +433,28 @@ struct Helmholtz {
     }
 };
 
-// One implicit-Euler step of the transient plate heat problem
-// (apps/welding/src/level2_transient_heat.cpp:237-292): screened Poisson with
-// alpha = 1/sqrt(kappa dt), zero boundary data and the source
-//   alpha^2 max(0, u_prev(x)) + fraction * q_v(x) / k,
-// u_prev read from the previous step's grid field by the reference's
-// FieldSampler2D (apps/welding/include/welding/field_sampler.hpp:32-126) and
-// q_v the finite-plate Gaussian power density of
-// apps/welding/include/welding/gaussian_heat_source.hpp:38-41, 112-123.
+// One implicit-Euler step of the reference's transient plate problems:
+// screened Poisson with alpha = 1/sqrt(kappa dt), zero boundary data and a
+// source built from the previous step's grid field u_prev, read by the
+// reference's FieldSampler2D (apps/welding/include/welding/field_sampler.hpp:
+// 32-126).  Sources, by `kind`:
+//   0  alpha^2 u_prev                       cooling (apps/welding/src/level0_cooling.cpp:194-196)
+//   2  alpha^2 max(0, u_prev) + fraction q_v / k   stationary Gaussian
+//      (level2_transient_heat.cpp:251-259, q_v from gaussian_heat_source.hpp:38-41)
+//   3  alpha^2 max(0, u_prev) + q_m / k     moving Gaussian, two Gauss-Legendre
+//      components per step (level3_moving_heat.cpp:189-194,
+//      moving_gaussian_heat_source.hpp:73-88)
 // Expression order follows the reference (the exact path rounds like it).
 struct TransientDesc {
     double alpha;
-    double fraction;       // share of the step with the heat source on
+    double fraction;       // kind 2: share of the step with the heat source on
     double conductivity;
-    double power;          // absorbed power
-    double thickness, ix, iy;  // plate thickness, Gaussian integrals over x and y
-    double cx, cy, sx, sy;
+    double power;          // kind 2: absorbed power
+    double thickness, ix, iy;  // kind 2: plate thickness, Gaussian integrals over x and y
+    double cx, cy, sx, sy;     // kind 2: centre and widths
+    int kind;
+    int moving;            // kind 3: 2 when the source is on during the step, else 0
+    double mx[2], my[2], mcoef[2];  // kind 3: component centres and coefficients
     const double *prev;    // previous field, (i, j) row-major, nx * ny
     int nx, ny;
     double xmin, xmax, ymin, ymax;
@@ -508,10 +514,20 @@ __device__ __forceinline__ double field_sample(const TransientDesc &t, double x,
     return (1.0 - ty) * lower + ty * upper;
 }
 
-// TransientGaussianHeat2D::source
+// The equations' source(point)
 __device__ __forceinline__ double transient_source(const TransientDesc &t, double x, double y) {
     const double v = field_sample(t, x, y);
+    if (t.kind == 0) return t.alpha * t.alpha * v;
     const double previous = t.alpha * t.alpha * (0.0 < v ? v : 0.0);
+    if (t.kind == 3) {
+        double value = 0.0;
+        for (int k = 0; k < t.moving; ++k) {
+            const double dx = (x - t.mx[k]) / t.sx;
+            const double dy = (y - t.my[k]) / t.sy;
+            value += t.mcoef[k] * exp(-0.5 * (dx * dx + dy * dy));
+        }
+        return previous + value / t.conductivity;
+    }
     double heat = 0.0;
     if (t.fraction > 0.0) {
         const double dx = (x - t.cx) / t.sx;

@@ -46,15 +46,24 @@ int step_count(const wos_transient_params &p) {
 // The reference's checks (level2_transient_heat.cpp:206-223 and the source's
 // constructor, gaussian_heat_source.hpp:28-36), with its messages.
 std::string check(const wos_transient_params &p) {
+    if (p.scenario != 0 && p.scenario != 2 && p.scenario != 3) return "scenario must be 0, 2 or 3";
     if (p.nx < 3 || p.ny < 3 || p.nx % 2 == 0 || p.ny % 2 == 0) {
         return "--nx and --ny must be odd integers of at least 3";
     }
-    if (!(p.dt > 0.0) || !(p.total_time > 0.0) || !(p.heat_on_time > 0.0) ||
-        !(p.epsilon > 0.0) || p.walks < 1 || p.max_steps < 1) {
+    if (!(p.dt > 0.0) || !(p.total_time > 0.0) || !(p.epsilon > 0.0) || p.walks < 1 ||
+        p.max_steps < 1 || (p.scenario != 0 && !(p.heat_on_time > 0.0))) {
         return "dt, total_time, heat_on_time, epsilon, walks and max_steps must be positive";
     }
-    if (!(p.heat_on_time < p.total_time)) {
+    if (p.scenario == 2 && !(p.heat_on_time < p.total_time)) {
         return "--heat-on-time must be smaller than --total-time";
+    }
+    if (!std::isfinite(p.plate_x0) || !std::isfinite(p.plate_y0)) {
+        return "plate corner must be finite";
+    }
+    if (p.scenario == 3 &&
+        (!(p.weld_speed > 0.0) || p.weld_y < p.plate_y0 || p.weld_y > p.plate_y0 + p.length_y)) {
+        // moving_gaussian_heat_source.hpp:21-28
+        return "invalid moving Gaussian parameters";
     }
     const double steps = p.total_time / p.dt;
     if (std::abs(steps - std::round(steps)) > 1e-10 * std::max(1.0, steps)) {
@@ -63,9 +72,10 @@ std::string check(const wos_transient_params &p) {
     if (!(p.epsilon < 0.5 * std::min(p.length_x, p.length_y))) {
         return "--epsilon is too large for the plate";
     }
-    if (!(p.length_x > 0.0) || !(p.length_y > 0.0) || !(p.thickness > 0.0) ||
-        !(p.electrical_power > 0.0) || !(p.efficiency > 0.0) || p.efficiency > 1.0 ||
-        !(p.sigma_x > 0.0) || !(p.sigma_y > 0.0)) {
+    if (!(p.length_x > 0.0) || !(p.length_y > 0.0)) return "invalid plate size";
+    if (p.scenario != 0 &&
+        (!(p.thickness > 0.0) || !(p.electrical_power > 0.0) || !(p.efficiency > 0.0) ||
+         p.efficiency > 1.0 || !(p.sigma_x > 0.0) || !(p.sigma_y > 0.0))) {
         return "invalid Gaussian heat-source parameters";
     }
     if (!(p.conductivity > 0.0) || !(p.density > 0.0) || !(p.specific_heat > 0.0)) {
@@ -102,6 +112,13 @@ extern "C" void wos_transient_defaults(wos_transient_params *p) {
     p->sigma_x = 0.006;
     p->sigma_y = 0.006;
     p->method = WOS_METHOD_FAST_FP32;
+    p->scenario = 2;
+    p->plate_x0 = -0.5 * p->length_x;
+    p->plate_y0 = -0.5 * p->length_y;
+    // Level3Config (level3_moving_heat.cpp:64-67)
+    p->weld_y = 0.0;
+    p->source_start_x = -0.05;
+    p->weld_speed = 0.02;
 }
 
 extern "C" int wos_transient_steps(const wos_transient_params *p) {
@@ -110,8 +127,9 @@ extern "C" int wos_transient_steps(const wos_transient_params *p) {
 }
 
 extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params *pp,
-                                   int use_graph, double *fields, double *standard_error,
-                                   long long *max_steps_hits, float *device_ms) {
+                                   const double *initial, int use_graph, double *fields,
+                                   double *standard_error, long long *max_steps_hits,
+                                   float *device_ms) {
     if (!ctx) return fail(nullptr, WOS_ERR_INVALID, "null context");
     if (!pp) return fail(ctx, WOS_ERR_INVALID, "wos_transient_solve: null params");
     const wos_transient_params &p = *pp;
@@ -121,8 +139,8 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
     cudaStream_t stream = ctx->stream;
 
     // the plate (rectangular_plate.hpp:11-34) and its grid
-    const double xmin = -0.5 * p.length_x, xmax = 0.5 * p.length_x;
-    const double ymin = -0.5 * p.length_y, ymax = 0.5 * p.length_y;
+    const double xmin = p.plate_x0, xmax = p.plate_x0 + p.length_x;
+    const double ymin = p.plate_y0, ymax = p.plate_y0 + p.length_y;
     const double verts[8] = {xmin, ymin, xmax, ymin, xmax, ymax, xmin, ymax};
     const int prims[8] = {0, 1, 1, 2, 2, 3, 3, 0};
     const int bids[4] = {0, 0, 0, 0};
@@ -163,6 +181,11 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
     WOS_CUDA(ctx, d_desc.reserve(sizeof(TransientDesc) * steps), "alloc step descriptors");
     WOS_CUDA(ctx, cudaMemsetAsync(d_fields.ptr, 0, field_bytes, stream), "clear fields");
     WOS_CUDA(ctx, cudaMemsetAsync(d_se.ptr, 0, field_bytes, stream), "clear fields");
+    if (initial) {
+        WOS_CUDA(ctx, cudaMemcpyAsync(d_fields.ptr, initial, sizeof(double) * n,
+                                      cudaMemcpyHostToDevice, stream),
+                 "H2D initial field");
+    }
     WOS_CUDA(ctx, cudaMemsetAsync(d_ctr.ptr, 0, sizeof(DeviceCounters) * (steps + 1), stream),
              "clear counters");
     auto *fld = static_cast<double *>(d_fields.ptr);
@@ -175,21 +198,57 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
     // physical constants (level2_transient_heat.cpp:404-409, 430-436)
     const double diffusivity = p.conductivity / (p.density * p.specific_heat);
     const double alpha = 1.0 / std::sqrt(diffusivity * p.dt);
-    const double ix = gaussian_integral(xmin, xmax, 0.0, p.sigma_x);
-    const double iy = gaussian_integral(ymin, ymax, 0.0, p.sigma_y);
+    // the stationary source sits at the plate centre
+    const double cx = 0.5 * (xmin + xmax), cy = 0.5 * (ymin + ymax);
+    const double ix = p.scenario == 2 ? gaussian_integral(xmin, xmax, cx, p.sigma_x) : 0.0;
+    const double iy = p.scenario == 2 ? gaussian_integral(ymin, ymax, cy, p.sigma_y) : 0.0;
     std::vector<TransientDesc> host(steps);
     for (int s = 1; s <= steps; ++s) {
         TransientDesc &t = host[s - 1];
         t = TransientDesc{};
+        t.kind = p.scenario;
         t.alpha = alpha;
-        t.fraction = heating_fraction((s - 1) * p.dt, s * p.dt, p.heat_on_time);
+        t.fraction = p.scenario == 2
+                         ? heating_fraction((s - 1) * p.dt, s * p.dt, p.heat_on_time)
+                         : 0.0;
         t.conductivity = p.conductivity;
         t.power = p.electrical_power * p.efficiency;
         t.thickness = p.thickness;
         t.ix = ix;
         t.iy = iy;
-        t.cx = 0.0;
-        t.cy = 0.0;
+        t.cx = cx;
+        t.cy = cy;
+        if (p.scenario == 3) {
+            // MovingGaussianStepSource2D (moving_gaussian_heat_source.hpp:16-71)
+            const double time_begin = (s - 1) * p.dt, time_end = s * p.dt;
+            const double active_begin = std::max(0.0, time_begin);
+            const double active_end = std::min(time_end, p.heat_on_time);
+            t.moving = 0;
+            if (active_end > active_begin) {
+                const double active_fraction =
+                    (active_end - active_begin) / (time_end - time_begin);
+                const double midpoint = 0.5 * (active_begin + active_end);
+                const double half_width = 0.5 * (active_end - active_begin);
+                constexpr double inverse_sqrt_three = 0.577350269189625764509148780501957456;
+                const double times[2] = {midpoint - inverse_sqrt_three * half_width,
+                                         midpoint + inverse_sqrt_three * half_width};
+                const double absorbed = p.electrical_power * p.efficiency;
+                for (int k = 0; k < 2; ++k) {
+                    const double mx = p.source_start_x + p.weld_speed * times[k];
+                    if (mx < xmin || mx > xmax) {
+                        return fail(ctx, WOS_ERR_INVALID,
+                                    "wos_transient_solve: moving Gaussian centre leaves the "
+                                    "finite plate");
+                    }
+                    const double gx = gaussian_integral(xmin, xmax, mx, p.sigma_x);
+                    const double gy = gaussian_integral(ymin, ymax, p.weld_y, p.sigma_y);
+                    t.mx[k] = mx;
+                    t.my[k] = p.weld_y;
+                    t.mcoef[k] = active_fraction * absorbed / (2.0 * p.thickness * gx * gy);
+                }
+                t.moving = 2;
+            }
+        }
         t.sx = p.sigma_x;
         t.sy = p.sigma_y;
         t.prev = fld + static_cast<size_t>(s - 1) * n;
