@@ -32,6 +32,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import time
 import sys
 
 import numpy as np
@@ -195,10 +196,13 @@ def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
     s = Solver(device)
     b = Batch(s)
     built = []
+    host_build_s = 0.0
     for sp in specs:
         mesh = build_mesh(sp["mesh"])
         built.append(mesh)
-        mid = b.add_mesh(mesh)
+        t0 = time.perf_counter()
+        mid = b.add_mesh(mesh)          # BVH build on the host threads + upload
+        host_build_s += time.perf_counter() - t0
         b.add_solve(mid, sp["equation"], *sp["grid"], **sp["params"])
     b.run(use_graph=True)            # plan, capture, warm
     ms = b.run(use_graph=True)
@@ -206,6 +210,7 @@ def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
     out = {"workload": "mixed_batch_64", "scale": scale, "solves": info["solves"],
            "points": info["points"], "walks": info["walks"], "steps": info["steps"],
            "prims": [int(m.prims.shape[0]) for m in built],
+           "host_build_and_upload_s": host_build_s,
            "batch_graph_ms": ms, "batch_walks_per_s": info["walks"] / (ms / 1000.0),
            "batch_queries_per_s": info["steps"] / (ms / 1000.0)}
     ms_stream = b.run(use_graph=False)

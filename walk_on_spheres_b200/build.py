@@ -33,7 +33,7 @@ CXX = os.environ.get("CXX", "g++")
 
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter",
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-pthread", "-Wall", "-Wextra", "-Wno-unused-parameter",
              "-I", str(CUDA_HOME / "include"), "-I", str(INCLUDE), "-I", str(CSRC)]
 
 CUDA_UNITS = {

@@ -5,10 +5,57 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 namespace wosb {
 
 namespace {
+
+// Subtree recursions split into host threads down to this depth (2^depth
+// threads at most); below it, or under kSerialItems items, they run inline.
+// Subtrees touch disjoint item ranges and node slots, so the result does not
+// depend on the thread count.
+int spawn_depth() {
+    static const int d = [] {
+        unsigned hw = std::thread::hardware_concurrency();
+        int k = 0;
+        while ((2u << k) <= std::max(1u, hw) && k < 6) ++k;
+        return k;
+    }();
+    return d;
+}
+constexpr int kSerialItems = 8192;
+
+template <class F, class G>
+void both(int depth, int items, F &&left, G &&right) {
+    if (depth < spawn_depth() && items >= kSerialItems) {
+        std::thread t(std::forward<F>(left));
+        right();
+        t.join();
+    } else {
+        left();
+        right();
+    }
+}
+
+// Runs f(i) for i in [0, n) on the host threads, in contiguous blocks.
+template <class F>
+void parallel_for(long long n, F &&f) {
+    const long long threads = std::max(1u, std::thread::hardware_concurrency());
+    if (n < 64 || threads == 1) {
+        for (long long i = 0; i < n; ++i) f(i);
+        return;
+    }
+    const long long per = (n + threads - 1) / threads;
+    std::vector<std::thread> pool;
+    for (long long b = 0; b < n; b += per) {
+        const long long e = std::min(n, b + per);
+        pool.emplace_back([&f, b, e] {
+            for (long long i = b; i < e; ++i) f(i);
+        });
+    }
+    for (auto &t : pool) t.join();
+}
 
 struct Item {
     double lo[3], hi[3], c[3];
@@ -82,8 +129,8 @@ struct Builder {
                              if (x.c[axis] > y.c[axis]) return false;
                              return x.prim < y.prim;
                          });
-        build(2 * id, level + 1, s, mid);
-        build(2 * id + 1, level + 1, mid, e);
+        both(level, e - s, [&] { build(2 * id, level + 1, s, mid); },
+             [&] { build(2 * id + 1, level + 1, mid, e); });
     }
 };
 
@@ -107,10 +154,10 @@ struct WideBuilder {
         }
     }
 
-    void split(int s, int e, long long chunk, int child_height) {
+    void split(int s, int e, long long chunk, int child_height, int depth = 0) {
         const long long nch = (e - s + chunk - 1) / chunk;
         if (nch <= 1) {
-            node(s, e, child_height);
+            node(s, e, child_height, depth);
             return;
         }
         const int mid = static_cast<int>(s + ((nch + 1) / 2) * chunk);
@@ -125,11 +172,11 @@ struct WideBuilder {
                              if (x.c[axis] > y.c[axis]) return false;
                              return x.prim < y.prim;
                          });
-        split(s, mid, chunk, child_height);
-        split(mid, e, chunk, child_height);
+        both(depth, e - s, [&] { split(s, mid, chunk, child_height, depth + 1); },
+             [&] { split(mid, e, chunk, child_height, depth + 1); });
     }
 
-    void node(int s, int e, int height) {
+    void node(int s, int e, int height, int depth = 0) {
         if (height <= 1) {
             std::sort(items.begin() + s, items.begin() + e,
                       [](const Item &x, const Item &y) { return x.prim < y.prim; });
@@ -137,7 +184,7 @@ struct WideBuilder {
         }
         long long chunk = 1;
         for (int h = 1; h < height; ++h) chunk *= 32;
-        split(s, e, chunk, height - 1);
+        split(s, e, chunk, height - 1, depth);
     }
 };
 
@@ -282,11 +329,11 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
         const int v = sc.prims[static_cast<size_t>(dim) * prim + j];
         for (int k = 0; k < dim; ++k) out[k] = sc.verts[static_cast<size_t>(dim) * v + k];
     };
-    std::vector<double> pts;
     for (int h = 1; h < H; ++h) {
         long long span_h = 1;
         for (int k = 0; k < h; ++k) span_h *= 32;
-        for (long long i = 0; i < cnt[h]; ++i) {
+        parallel_for(cnt[h], [&](long long i) {
+            std::vector<double> pts;
             float *blk = sc.wbox.data() + sc.w_off[h] + static_cast<size_t>(i / 32) * nbox * 32;
             const int lane = static_cast<int>(i % 32);
             for (int k = 0; k < nc; ++k) {
@@ -319,7 +366,7 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
             for (int k = 0; k < dim; ++k) blk[(nc + k) * 32 + lane] = nf[k];
             blk[(nc + dim) * 32 + lane] = cf;
             blk[(nc + dim + 1) * 32 + lane] = round_up(t32 + 4.0 * widen);
-        }
+        });
     }
     // primitives in wide-slot order, one block of na x 32 floats per cluster
     // (field f of slot 32c + k at c*na*32 + f*32 + k); padding primitives are
