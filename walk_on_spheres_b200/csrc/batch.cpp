@@ -42,7 +42,7 @@ struct BatchSolve {
 };
 
 struct Family {
-    int dim, kind, precision;
+    int dim, kind, precision, hc;
     int first, count;  // items
     long long n_tasks;
     int blocks;
@@ -113,7 +113,8 @@ int wos_batch::plan() {
         const BatchSolve &b = solves[s];
         const int dim = meshes[b.mesh]->scene.dim;
         const int prec = b.p.method == WOS_METHOD_FAST_FP32 ? 0 : 1;
-        return (dim * 8 + b.p.equation) * 2 + prec;
+        const int hc = prec == 0 ? height_class(meshes[b.mesh]->dev.wide.H) + 1 : 0;
+        return ((dim * 8 + b.p.equation) * 2 + prec) * 8 + hc;
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
 
@@ -194,9 +195,11 @@ int wos_batch::plan() {
         it.max_ray_attempts = b.p.max_ray_attempts;
         it.precision = precision;
         it.point_begin = b.point_begin;
+        const int hc = precision == 32 ? height_class(m.dev.wide.H) : kHeightAny;
         if (families.empty() || families.back().dim != dim ||
-            families.back().kind != b.p.equation || families.back().precision != precision) {
-            families.push_back(Family{dim, b.p.equation, precision, i, 0, 0, 0});
+            families.back().kind != b.p.equation || families.back().precision != precision ||
+            families.back().hc != hc) {
+            families.push_back(Family{dim, b.p.equation, precision, hc, i, 0, 0, 0});
         }
         Family &f = families.back();
         it.task_begin = f.n_tasks;
@@ -207,7 +210,7 @@ int wos_batch::plan() {
         if (blocks_override > 0) {
             f.blocks = blocks_override;
         } else {
-            WOS_CUDA(ctx, batch_walk_blocks(f.dim, f.kind, f.precision, &f.blocks),
+            WOS_CUDA(ctx, batch_walk_blocks(f.dim, f.kind, f.precision, f.hc, &f.blocks),
                      "batch occupancy");
         }
     }
@@ -240,7 +243,7 @@ cudaError_t wos_batch::enqueue() {
     if (e != cudaSuccess) return e;
     for (size_t f = 0; f < families.size(); ++f) {
         const Family &fam = families[f];
-        e = launch_walk_batch(fam.dim, fam.kind, fam.precision, di + fam.first, fam.count,
+        e = launch_walk_batch(fam.dim, fam.kind, fam.precision, fam.hc, di + fam.first, fam.count,
                               fam.n_tasks, q + f, fam.blocks, s);
         if (e != cudaSuccess) return e;
     }

@@ -26,6 +26,7 @@
 // Nearest32 in scene.cuh): bound = best * keep while best > exact2.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 namespace wosb {
 
@@ -100,9 +101,29 @@ __device__ __forceinline__ float wide_prim_dist(const WideView &w, int cluster, 
     return eberly32(px, py, pz, rec);
 }
 
+// Height classes of the traversal: a kernel compiled for one class carries
+// only that class's code (the other paths cost registers and instruction
+// cache on the hot ones).  kHeightAny keeps every path.
+enum : int { kHeightAny = -1, kHeightOther = 0, kHeightUpTo2 = 2, kHeight3 = 3 };
+
+__host__ __device__ __forceinline__ int height_class(int H) {
+    return H <= 2 ? kHeightUpTo2 : (H == 3 ? kHeight3 : kHeightOther);
+}
+
+// Host dispatch: calls f(std::integral_constant<int, HC>{}) for class hc.
+template <class F>
+inline auto with_height_class(int hc, F &&f) {
+    switch (hc) {
+        case kHeightUpTo2: return f(std::integral_constant<int, kHeightUpTo2>{});
+        case kHeight3: return f(std::integral_constant<int, kHeight3>{});
+        default: return f(std::integral_constant<int, kHeightOther>{});
+    }
+}
+
 // Closest primitive to (px, py, pz); all 32 lanes of the warp must call this
-// with the same point and receive the same result.
-template <int DIM>
+// with the same point and receive the same result.  HC: the height class the
+// caller guarantees (height_class(w.H) == HC), or kHeightAny.
+template <int DIM, int HC = kHeightAny>
 __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, float py,
                                                    float pz, float keep, float exact2) {
     constexpr unsigned kAll = 0xffffffffu;
@@ -125,6 +146,7 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         m &= ~(1u << k);
         return k;
     };
+    if constexpr (HC == kHeightUpTo2 || HC == kHeightAny) {
     if (w.H == 1) {
         leaf(0);
         return WideResult{best, slot};
@@ -140,8 +162,10 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         }
         return WideResult{best, slot};
     }
+    }
     // Heights 3 and 4: the same nearest-first order with one child bound per
     // level held in a register, so going back up re-reads nothing.
+    if constexpr (HC == kHeight3 || HC == kHeightAny) {
     if (w.H == 3) {
         const float d2 = wide_box_dist<DIM>(w, 2, 0, px, py, pz);
         unsigned m2 = __ballot_sync(kAll, d2 < limit);
@@ -158,6 +182,8 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         }
         return WideResult{best, slot};
     }
+    }
+    if constexpr (HC == kHeightOther || HC == kHeightAny) {
     if (w.H == 4) {
         const float d3 = wide_box_dist<DIM>(w, 3, 0, px, py, pz);
         unsigned m3 = __ballot_sync(kAll, d3 < limit);
@@ -208,6 +234,7 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
             d = wide_box_dist<DIM>(w, h - 1, node, px, py, pz);
             m = __ballot_sync(kAll, d < limit);
         }
+    }
     }
     return WideResult{best, slot};
 }

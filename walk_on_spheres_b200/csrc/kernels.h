@@ -100,13 +100,14 @@ struct BatchItem {
 cudaError_t launch_classify_batch(int dim, const BatchItem *items, int n_items,
                                   long long point_base, long long n_points, cudaStream_t stream);
 
-// Fast walks of one family (all items share dim, equation kind and
-// precision; tasks numbered by task_begin from 0) on a persistent grid of
-// `blocks` blocks (batch_walk_blocks: every block that can be resident).
-cudaError_t launch_walk_batch(int dim, int kind, int precision, const BatchItem *items,
+// Fast walks of one family (all items share dim, equation kind, precision
+// and, for precision 32, the wide tree's height class `hc`; tasks numbered
+// by task_begin from 0) on a persistent grid of `blocks` blocks
+// (batch_walk_blocks: every block that can be resident).
+cudaError_t launch_walk_batch(int dim, int kind, int precision, int hc, const BatchItem *items,
                               int n_items, long long n_tasks, unsigned long long *queue,
                               int blocks, cudaStream_t stream);
-cudaError_t batch_walk_blocks(int dim, int kind, int precision, int *blocks);
+cudaError_t batch_walk_blocks(int dim, int kind, int precision, int hc, int *blocks);
 
 // Per-point merge of every item of the batch.
 cudaError_t launch_merge_batch(const BatchItem *items, int n_items, long long n_points,

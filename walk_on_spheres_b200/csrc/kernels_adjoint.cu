@@ -208,7 +208,7 @@ __device__ __forceinline__ double heat_source(const HeatArgs &a, V3<T> p, T R, F
     return mf;
 }
 
-template <int DIM, typename T, int MIN_BLOCKS>
+template <int DIM, typename T, int MIN_BLOCKS, int HC>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) {
     constexpr bool kF32 = std::is_same<T, float>::value;
     extern __shared__ float4 smem[];
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                     const float qy = __shfl_sync(kFull, static_cast<float>(p.y), jl);
                     const float qz =
                         DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), jl) : 0.0f;
-                    const WideResult r = wide_nearest<DIM>(wv, qx, qy, qz, a.keep, a.exact2);
+                    const WideResult r = wide_nearest<DIM, HC>(wv, qx, qy, qz, a.keep, a.exact2);
                     if (lane == jl) {
                         qbest = r.best;
                         qslot = r.slot;
@@ -537,19 +537,24 @@ cudaError_t launch_heat_dim(const HeatArgs &a, int precision, const FastPlan &pl
     };
     int blocks = 0;
     if (precision == 32) {
-        auto k = heat_walk_kernel<DIM, float, 3>;
-        // the static accumulators (20 KB) plus the staged scene can pass the
-        // 48 KB default: opt in whenever anything is staged
-        if (plan.smem_bytes > 0) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 plan.smem_bytes);
+        // forward and replay read the same tree, so they use one instantiation
+        return with_height_class(height_class(a.w.H), [&](auto h) -> cudaError_t {
+            constexpr int HC = decltype(h)::value;
+            auto k = heat_walk_kernel<DIM, float, 3, HC>;
+            // the static accumulators (20 KB) plus the staged scene can pass
+            // the 48 KB default: opt in whenever anything is staged
+            if (plan.smem_bytes > 0) {
+                cudaError_t e = cudaFuncSetAttribute(
+                    k, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem_bytes);
+                if (e != cudaSuccess) return e;
+            }
+            cudaError_t e = grid_for(k, plan.smem_bytes, blocks);
             if (e != cudaSuccess) return e;
-        }
-        cudaError_t e = grid_for(k, plan.smem_bytes, blocks);
-        if (e != cudaSuccess) return e;
-        k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a);
+            k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a);
+            return cudaGetLastError();
+        });
     } else {
-        auto k = heat_walk_kernel<DIM, double, 1>;
+        auto k = heat_walk_kernel<DIM, double, 1, kHeightAny>;
         cudaError_t e = grid_for(k, 0, blocks);
         if (e != cudaSuccess) return e;
         k<<<blocks, plan.threads, 0, stream>>>(a);

@@ -31,7 +31,7 @@ namespace {
 
 // One task: walks [c*chunk, min(N, (c+1)*chunk)) of point pidx, written to
 // a.partials[task] as Welford statistics.
-template <int DIM, class Eq, typename T>
+template <int DIM, class Eq, typename T, int HC>
 __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, const Eq &eq,
                                           unsigned long long task, long long pidx, int c) {
     constexpr bool kF32 = std::is_same<T, float>::value;
@@ -144,7 +144,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 const float qx = __shfl_sync(kFull, static_cast<float>(p.x), j);
                 const float qy = __shfl_sync(kFull, static_cast<float>(p.y), j);
                 const float qz = DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), j) : 0.0f;
-                const WideResult r = wide_nearest<DIM>(wv, qx, qy, qz, a.keep, a.exact2);
+                const WideResult r = wide_nearest<DIM, HC>(wv, qx, qy, qz, a.keep, a.exact2);
                 if (lane == j) {
                     qbest = r.best;
                     qslot = r.slot;
@@ -227,7 +227,7 @@ __device__ __forceinline__ Helmholtz<DIM> eq_from(const EqDesc &, Helmholtz<DIM>
     return Helmholtz<DIM>{};
 }
 
-template <int DIM, class Eq, typename T, int MIN_BLOCKS>
+template <int DIM, class Eq, typename T, int MIN_BLOCKS, int HC>
 __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, Eq eq) {
     constexpr bool kF32 = std::is_same<T, float>::value;
     extern __shared__ float4 smem[];
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, 
         const long long pidx = static_cast<long long>(task / a.chunks);
         const int c = static_cast<int>(task % a.chunks);
         if (a.location[pidx] != 1) continue;
-        fast_task<DIM, Eq, T>(a, wv, eq, task, pidx, c);
+        fast_task<DIM, Eq, T, HC>(a, wv, eq, task, pidx, c);
     }
 }
 
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, 
 // (numbered by task_begin); each task runs the walk_fast_kernel task body
 // with its own item's scene, grid, equation and statistics buffers (the
 // scene is read through L1/L2, never staged).
-template <int DIM, class Eq, typename T, int MIN_BLOCKS>
+template <int DIM, class Eq, typename T, int MIN_BLOCKS, int HC>
 __global__ void __launch_bounds__(256, MIN_BLOCKS)
     walk_batch_kernel(const BatchItem *__restrict__ items, int n_items, long long n_tasks,
                       unsigned long long *queue) {
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS)
         WideView wv = it.a.w;
         wv.off = s_off[warp];
         const Eq eq = eq_from(it.eq, static_cast<Eq *>(nullptr));
-        fast_task<DIM, Eq, T>(it.a, wv, eq, static_cast<unsigned long long>(local), pidx, c);
+        fast_task<DIM, Eq, T, HC>(it.a, wv, eq, static_cast<unsigned long long>(local), pidx, c);
     }
 }
 
@@ -357,26 +357,36 @@ __global__ void merge_batch_kernel(const BatchItem *__restrict__ items, int n_it
 }
 
 template <int DIM, class Eq>
-cudaError_t batch_typed(int precision, const BatchItem *items, int n_items, long long n_tasks,
-                        unsigned long long *queue, int blocks, cudaStream_t stream) {
+cudaError_t batch_typed(int precision, int hc, const BatchItem *items, int n_items,
+                        long long n_tasks, unsigned long long *queue, int blocks,
+                        cudaStream_t stream) {
     if (precision == 32) {
-        walk_batch_kernel<DIM, Eq, float, 3><<<blocks, 256, 0, stream>>>(items, n_items, n_tasks,
-                                                                         queue);
-    } else {
-        walk_batch_kernel<DIM, Eq, double, 1><<<blocks, 256, 0, stream>>>(items, n_items,
-                                                                          n_tasks, queue);
+        return with_height_class(hc, [&](auto h) {
+            constexpr int HC = decltype(h)::value;
+            walk_batch_kernel<DIM, Eq, float, 3, HC><<<blocks, 256, 0, stream>>>(
+                items, n_items, n_tasks, queue);
+            return cudaGetLastError();
+        });
     }
+    walk_batch_kernel<DIM, Eq, double, 1, kHeightAny><<<blocks, 256, 0, stream>>>(
+        items, n_items, n_tasks, queue);
     return cudaGetLastError();
 }
 
 template <int DIM, class Eq>
-cudaError_t batch_blocks_typed(int precision, int &blocks) {
+cudaError_t batch_blocks_typed(int precision, int hc, int &blocks) {
     int per_sm = 0, dev = 0, sms = 0;
-    cudaError_t e = precision == 32
-                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &per_sm, walk_batch_kernel<DIM, Eq, float, 3>, 256, 0)
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &per_sm, walk_batch_kernel<DIM, Eq, double, 1>, 256, 0);
+    cudaError_t e;
+    if (precision == 32) {
+        e = with_height_class(hc, [&](auto h) {
+            constexpr int HC = decltype(h)::value;
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, walk_batch_kernel<DIM, Eq, float, 3, HC>, 256, 0);
+        });
+    } else {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, walk_batch_kernel<DIM, Eq, double, 1, kHeightAny>, 256, 0);
+    }
     if (e != cudaSuccess) return e;
     e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -387,26 +397,30 @@ cudaError_t batch_blocks_typed(int precision, int &blocks) {
 }
 
 template <int DIM>
-cudaError_t batch_dispatch(int kind, int precision, const BatchItem *items, int n_items,
+cudaError_t batch_dispatch(int kind, int precision, int hc, const BatchItem *items, int n_items,
                            long long n_tasks, unsigned long long *queue, int blocks,
                            cudaStream_t stream, int *blocks_out) {
     switch (kind) {
         case kLaplace:
-            return blocks_out ? batch_blocks_typed<DIM, Laplace<DIM>>(precision, *blocks_out)
-                              : batch_typed<DIM, Laplace<DIM>>(precision, items, n_items, n_tasks,
-                                                               queue, blocks, stream);
+            return blocks_out
+                       ? batch_blocks_typed<DIM, Laplace<DIM>>(precision, hc, *blocks_out)
+                       : batch_typed<DIM, Laplace<DIM>>(precision, hc, items, n_items, n_tasks,
+                                                        queue, blocks, stream);
         case kPoisson:
-            return blocks_out ? batch_blocks_typed<DIM, Poisson<DIM>>(precision, *blocks_out)
-                              : batch_typed<DIM, Poisson<DIM>>(precision, items, n_items, n_tasks,
-                                                               queue, blocks, stream);
+            return blocks_out
+                       ? batch_blocks_typed<DIM, Poisson<DIM>>(precision, hc, *blocks_out)
+                       : batch_typed<DIM, Poisson<DIM>>(precision, hc, items, n_items, n_tasks,
+                                                        queue, blocks, stream);
         case kScreened:
-            return blocks_out ? batch_blocks_typed<DIM, Screened<DIM>>(precision, *blocks_out)
-                              : batch_typed<DIM, Screened<DIM>>(precision, items, n_items,
-                                                                n_tasks, queue, blocks, stream);
+            return blocks_out
+                       ? batch_blocks_typed<DIM, Screened<DIM>>(precision, hc, *blocks_out)
+                       : batch_typed<DIM, Screened<DIM>>(precision, hc, items, n_items, n_tasks,
+                                                         queue, blocks, stream);
         default:
-            return blocks_out ? batch_blocks_typed<DIM, Helmholtz<DIM>>(precision, *blocks_out)
-                              : batch_typed<DIM, Helmholtz<DIM>>(precision, items, n_items,
-                                                                 n_tasks, queue, blocks, stream);
+            return blocks_out
+                       ? batch_blocks_typed<DIM, Helmholtz<DIM>>(precision, hc, *blocks_out)
+                       : batch_typed<DIM, Helmholtz<DIM>>(precision, hc, items, n_items, n_tasks,
+                                                          queue, blocks, stream);
     }
 }
 
@@ -495,17 +509,21 @@ cudaError_t launch_fast_typed(const FastArgs &a, const EqDesc &e, int precision,
     };
     int blocks = 0;
     if (precision == 32) {
-        auto k = walk_fast_kernel<DIM, Eq, float, 3>;
-        if (plan.smem_bytes > 48 * 1024) {
-            cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   plan.smem_bytes);
+        return with_height_class(height_class(a.w.H), [&](auto h) -> cudaError_t {
+            constexpr int HC = decltype(h)::value;
+            auto k = walk_fast_kernel<DIM, Eq, float, 3, HC>;
+            if (plan.smem_bytes > 48 * 1024) {
+                cudaError_t err = cudaFuncSetAttribute(
+                    k, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem_bytes);
+                if (err != cudaSuccess) return err;
+            }
+            cudaError_t err = grid_for(k, plan.smem_bytes, blocks);
             if (err != cudaSuccess) return err;
-        }
-        cudaError_t err = grid_for(k, plan.smem_bytes, blocks);
-        if (err != cudaSuccess) return err;
-        k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq_host<Eq>(e));
+            k<<<blocks, plan.threads, plan.smem_bytes, stream>>>(a, eq_host<Eq>(e));
+            return cudaGetLastError();
+        });
     } else {
-        auto k = walk_fast_kernel<DIM, Eq, double, 1>;
+        auto k = walk_fast_kernel<DIM, Eq, double, 1, kHeightAny>;
         cudaError_t err = grid_for(k, 0, blocks);
         if (err != cudaSuccess) return err;
         k<<<blocks, plan.threads, 0, stream>>>(a, eq_host<Eq>(e));
@@ -619,19 +637,21 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
     return cudaGetLastError();
 }
 
-cudaError_t batch_walk_blocks(int dim, int kind, int precision, int *blocks) {
-    return dim == 2 ? batch_dispatch<2>(kind, precision, nullptr, 0, 0, nullptr, 0, nullptr, blocks)
-                    : batch_dispatch<3>(kind, precision, nullptr, 0, 0, nullptr, 0, nullptr, blocks);
+cudaError_t batch_walk_blocks(int dim, int kind, int precision, int hc, int *blocks) {
+    return dim == 2 ? batch_dispatch<2>(kind, precision, hc, nullptr, 0, 0, nullptr, 0, nullptr,
+                                        blocks)
+                    : batch_dispatch<3>(kind, precision, hc, nullptr, 0, 0, nullptr, 0, nullptr,
+                                        blocks);
 }
 
-cudaError_t launch_walk_batch(int dim, int kind, int precision, const BatchItem *items,
+cudaError_t launch_walk_batch(int dim, int kind, int precision, int hc, const BatchItem *items,
                               int n_items, long long n_tasks, unsigned long long *queue,
                               int blocks, cudaStream_t stream) {
     if (n_items <= 0 || n_tasks <= 0) return cudaSuccess;
-    return dim == 2 ? batch_dispatch<2>(kind, precision, items, n_items, n_tasks, queue, blocks,
-                                        stream, nullptr)
-                    : batch_dispatch<3>(kind, precision, items, n_items, n_tasks, queue, blocks,
-                                        stream, nullptr);
+    return dim == 2 ? batch_dispatch<2>(kind, precision, hc, items, n_items, n_tasks, queue,
+                                        blocks, stream, nullptr)
+                    : batch_dispatch<3>(kind, precision, hc, items, n_items, n_tasks, queue,
+                                        blocks, stream, nullptr);
 }
 
 cudaError_t launch_merge_batch(const BatchItem *items, int n_items, long long n_points,
