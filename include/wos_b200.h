@@ -295,6 +295,59 @@ int wos_transient_solve(wos_context *ctx, const wos_transient_params *p, const d
                         int use_graph, double *fields, double *standard_error,
                         long long *max_steps_hits, float *device_ms);
 
+/* ------------------------------------------------ stationary plate heating */
+
+/* The reference's stationary welding program (apps/welding/src/
+ * level1_stationary_heat.cpp:132-269): -Lap u = f on the plate
+ * [0, length_x] x [0, length_y] with u = 0 on its edges, on an nx x ny grid
+ * whose edge points are boundary points (value 0) and whose interior points
+ * run `walks` walks each.
+ *   WOS_PLATE_MANUFACTURED  f = pi^2 (1/Lx^2 + 1/Ly^2) u*, with the exact
+ *                           solution u* = peak_rise sin(pi x/Lx) sin(pi y/Ly)
+ *                           (ManufacturedPoisson2D, :75-130)
+ *   WOS_PLATE_GAUSSIAN      f = q/k, q the Gaussian centred at
+ *                           (source_x, source_y) normalised on the finite
+ *                           plate (gaussian_heat_source.hpp)
+ *                           (StationaryGaussianHeat2D, :132-191)
+ * source_mode WOS_SOURCE_GREEN, WOS_SOURCE_UNIFORM or (Gaussian only)
+ * WOS_SOURCE_MIS: Green samples with probability mis_green_probability, else
+ * samples of the finite-plate Gaussian (include/wos/source_sampling.hpp:
+ * 35-78).  Seeds as the reference: splitmix64(seed ^ case_stream ^
+ * splitmix64(i*ny + j)); PLAIN_FP64 follows the reference's streams. */
+enum { WOS_PLATE_MANUFACTURED = 0, WOS_PLATE_GAUSSIAN = 1 };
+
+typedef struct {
+    int nx, ny;                /* >= 3 */
+    int walks, max_steps;
+    double epsilon;
+    uint64_t seed;
+    uint64_t case_stream;      /* the reference's per-case stream constant */
+    double length_x, length_y, thickness, conductivity;
+    double electrical_power, efficiency, sigma_x, sigma_y;
+    double source_x, source_y; /* Gaussian centre */
+    double peak_rise;          /* manufactured amplitude */
+    int source;                /* WOS_PLATE_* */
+    int source_mode;           /* WOS_SOURCE_* */
+    double mis_green_probability;
+    int method;                /* WOS_METHOD_* */
+    int max_proposal_attempts; /* rejection cap of the Gaussian proposal */
+} wos_stationary_params;
+
+/* The reference's Level1Config (:42-61) for `source`, with that case's
+ * stream constant and Green source sampling. */
+void wos_stationary_defaults(wos_stationary_params *p, int source);
+
+/* Solve on the context's device (the context's mesh is not used or
+ * changed).  mean / variance / standard_error / mean_steps (host, may be
+ * NULL): nx x ny doubles, index i*ny + j.  Parameter errors carry the
+ * reference's messages (gaussian_heat_source.hpp:28-36,
+ * source_sampling.hpp:41-47, wos.hpp:88-91); a proposal that found no plate
+ * point in max_proposal_attempts draws returns WOS_ERR_DEVICE with the
+ * reference's message (gaussian_heat_source.hpp:70-72). */
+int wos_stationary_solve(wos_context *ctx, const wos_stationary_params *p, double *mean,
+                         double *variance, double *standard_error, double *mean_steps,
+                         long long *max_steps_hits, float *device_ms);
+
 /* ------------------------------------ Gaussian heat source and its adjoint */
 
 /* Source of the differentiable heat problem (no reference counterpart; the

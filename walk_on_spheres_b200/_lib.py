@@ -74,6 +74,19 @@ class TransientParams(C.Structure):
                 ("weld_speed", C.c_double)]
 
 
+class StationaryParams(C.Structure):
+    """wos_stationary_params (the reference's Level1Config plus the case, source and method)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("walks", C.c_int), ("max_steps", C.c_int),
+                ("epsilon", C.c_double), ("seed", C.c_uint64), ("case_stream", C.c_uint64),
+                ("length_x", C.c_double), ("length_y", C.c_double), ("thickness", C.c_double),
+                ("conductivity", C.c_double), ("electrical_power", C.c_double),
+                ("efficiency", C.c_double), ("sigma_x", C.c_double), ("sigma_y", C.c_double),
+                ("source_x", C.c_double), ("source_y", C.c_double), ("peak_rise", C.c_double),
+                ("source", C.c_int), ("source_mode", C.c_int),
+                ("mis_green_probability", C.c_double), ("method", C.c_int),
+                ("max_proposal_attempts", C.c_int)]
+
+
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
                      C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double,
                      C.c_int)
@@ -110,6 +123,9 @@ SIGNATURES = {
     "wos_transient_steps": (C.c_int, [C.POINTER(TransientParams)]),
     "wos_transient_solve": (C.c_int, [VP, C.POINTER(TransientParams), VP, C.c_int, VP, VP,
                                       C.POINTER(C.c_longlong), C.POINTER(C.c_float)]),
+    "wos_stationary_defaults": (None, [C.POINTER(StationaryParams), C.c_int]),
+    "wos_stationary_solve": (C.c_int, [VP, C.POINTER(StationaryParams)] + [VP] * 4 +
+                             [C.POINTER(C.c_longlong), C.POINTER(C.c_float)]),
     "wos_batch_create": (C.c_int, [VP, C.POINTER(VP)]),
     "wos_batch_destroy": (None, [VP]),
     "wos_batch_add_mesh": (C.c_int, [VP, C.c_int, VP, C.c_int, VP, C.c_int, VP, C.c_int,

@@ -45,6 +45,7 @@ CUDA_UNITS = {
     "heat_api.cpp": ["-x", "cu"],
     "batch.cpp": ["-x", "cu"],
     "transient.cpp": ["-x", "cu"],
+    "stationary.cpp": ["-x", "cu"],
     "noalloc.cu": [],
 }
 HOST_UNITS = ["scene_build.cpp", "obj_reader.cpp", "runner.cpp", "h5_writer.cpp", "host_api.cpp"]

@@ -57,10 +57,12 @@ struct StartRecord {
 
 // Equation selection for runtime dispatch.
 struct EqDesc {
-    int kind;    // kLaplace ... kHelmholtz, kTransient (2D only)
-    int mode;    // kUniform / kGreen
+    int kind;    // kLaplace ... kHelmholtz, kTransient, kPlate (2D only)
+    int mode;    // kUniform / kGreen / kMis (kPlate only)
     double alpha;
     const TransientDesc *tr;  // kTransient: the step's descriptor (device memory)
+    const PlateDesc *pl;      // kPlate: the plate's descriptor (HOST memory, copied
+                              // into the kernel's equation at launch)
 };
 
 // Per-solve device counters (include/wos/runner.hpp:147-151).
@@ -93,7 +95,8 @@ __device__ __forceinline__ double boundary_value(const EqDesc &e, V3<double> p, 
         case kLaplace: return Laplace<DIM>{}.boundary(p, bid);
         case kPoisson: return Poisson<DIM>{e.mode, e.alpha}.boundary(p, bid);
         case kScreened: return Screened<DIM>{e.mode, e.alpha}.boundary(p, bid);
-        case kTransient: return 0.0;
+        case kTransient:
+        case kPlate: return 0.0;
         default: return Helmholtz<DIM>{}.boundary(p, bid);
     }
 }

@@ -19,7 +19,14 @@
 
 namespace wosb {
 
-enum : int { kLaplace = 0, kPoisson = 1, kScreened = 2, kHelmholtz = 3, kTransient = 4 };
+enum : int {
+    kLaplace = 0,
+    kPoisson = 1,
+    kScreened = 2,
+    kHelmholtz = 3,
+    kTransient = 4,
+    kPlate = 5
+};
 enum : int { kUniform = 0, kGreen = 1, kMis = 2 };
 
 template <typename T>
@@ -566,6 +573,136 @@ struct Transient {
     __device__ T screening(T R) const { return sc_weight_2d(static_cast<T>(alpha), R); }
 };
 
+// Stationary plate heating, the reference's welding level 1
+// (apps/welding/src/level1_stationary_heat.cpp:75-191): -Lap u = f on the
+// plate [xmin, xmax] x [ymin, ymax] with u = 0 on its edges.  Sources, by
+// `kind`:
+//   0  manufactured: lambda * peak sin(pi x / Lx) sin(pi y / Ly) with
+//      lambda = pi^2 (1/Lx^2 + 1/Ly^2) (ManufacturedPoisson2D, :75-103)
+//   1  Gaussian: q_v / k, q_v the finite-plate Gaussian
+//      (StationaryGaussianHeat2D, :132-191; gaussian_heat_source.hpp:38-41)
+// The Gaussian also supplies the Green-source MIS proposal: the finite-plate
+// Gaussian drawn by rejection from the untruncated normal
+// (gaussian_heat_source.hpp:54-73), density shape / (ix iy) on the plate
+// (:45-51).  Expression order follows the reference.
+struct PlateDesc {
+    int kind;
+    int max_attempts;          // proposal rejection cap (1e6 in the reference)
+    double peak, length_x, length_y, eigen;            // kind 0
+    double power, thickness, conductivity, ix, iy;     // kind 1
+    double cx, cy, sx, sy;
+    double beta;               // MIS: probability of a Green sample
+    double xmin, xmax, ymin, ymax;
+};
+
+__device__ __forceinline__ double plate_shape(const PlateDesc &d, double x, double y) {
+    const double dx = (x - d.cx) / d.sx;
+    const double dy = (y - d.cy) / d.sy;
+    return exp(-0.5 * (dx * dx + dy * dy));
+}
+
+__device__ __forceinline__ double plate_source(const PlateDesc &d, double x, double y) {
+    if (d.kind == 0) {
+        const double exact = d.peak * sin(kPi * x / d.length_x) * sin(kPi * y / d.length_y);
+        return d.eigen * exact;
+    }
+    const double density = d.power * plate_shape(d, x, y) / (d.thickness * d.ix * d.iy);
+    return density / d.conductivity;
+}
+
+template <int DIM>
+struct Plate {
+    static constexpr bool kSource = true, kScreening = false, kProposal = true;
+    int mode;  // kGreen, kUniform or (Gaussian only) kMis
+    PlateDesc d;
+    template <typename T>
+    __device__ T boundary(V3<T>, int) const { return T(0); }
+    template <typename T>
+    __device__ bool may_intersect(V3<T>, T) const { return true; }
+    template <typename T>
+    __device__ T source(V3<T> p) const {
+        return static_cast<T>(
+            plate_source(d, static_cast<double>(p.x), static_cast<double>(p.y)));
+    }
+    template <typename T>
+    __device__ T green(T R, T r) const { return pg_green_2d(R, r); }
+    template <typename T>
+    __device__ T green_mass(T R) const { return pg_mass_2d(R); }
+    template <typename T, class Rng>
+    __device__ T green_radius(T R, Rng &rng, bool &) const {
+        return pg_sample_radius_2d(R, rng);
+    }
+    template <typename T>
+    __device__ T screening(T) const { return T(1); }
+    __device__ double mis_green_probability() const { return d.beta; }
+    __device__ double proposal_pdf(double x, double y) const {
+        if (x < d.xmin || x > d.xmax || y < d.ymin || y > d.ymax) return 0.0;
+        return plate_shape(d, x, y) / (d.ix * d.iy);
+    }
+    // GaussianHeatSource2D::sample_spatial_distribution; sets `overflow`
+    // when every one of the max_attempts proposals fell off the plate.
+    template <bool EXACT, class Rng>
+    __device__ V3<double> proposal_sample(Rng &rng, bool &overflow) const {
+        constexpr double two_pi = 2.0 * kPi;
+        for (int attempt = 0; attempt < d.max_attempts; ++attempt) {
+            const double magnitude = sqrt(-2.0 * log(rng.unit64_open()));
+            const double u = rng.unit64();
+            double s, c;
+            if constexpr (EXACT) {
+                const double angle = two_pi * u;
+                c = cos(angle);
+                s = sin(angle);
+            } else {
+                sincospi(2.0 * u, &s, &c);
+            }
+            const V3<double> q{d.cx + d.sx * magnitude * c, d.cy + d.sy * magnitude * s, 0.0};
+            if (q.x >= d.xmin && q.x <= d.xmax && q.y >= d.ymin && q.y <= d.ymax) return q;
+        }
+        overflow = true;
+        return V3<double>{d.cx, d.cy, 0.0};
+    }
+};
+
+// Equations that carry a source proposal (kProposal) can run Green-source MIS.
+template <class Eq, class = void>
+struct HasProposal {
+    static constexpr bool value = false;
+};
+template <class Eq>
+struct HasProposal<Eq, decltype(void(Eq::kProposal))> {
+    static constexpr bool value = Eq::kProposal;
+};
+
+// One ball's Green-source MIS estimate with the balance heuristic over a
+// random mixture (include/wos/source_sampling.hpp:35-78): a Green sample
+// with probability beta, else a proposal sample; samples outside the ball
+// count zero.  The distances, densities and source are evaluated in FP64.
+template <int DIM, bool EXACT, typename T, class Eq, class Rng>
+__device__ __forceinline__ double mis_contribution(const Eq &eq, V3<T> p, T R, Rng &rng,
+                                                   bool &overflow) {
+    const double beta = eq.mis_green_probability();
+    V3<double> y;
+    if (static_cast<double>(rng.unit()) < beta) {
+        const T radius = eq.green_radius(R, rng, overflow);
+        const V3<T> g = direction_at<DIM, EXACT, T>(p, radius, rng);
+        y = V3<double>{static_cast<double>(g.x), static_cast<double>(g.y), 0.0};
+    } else {
+        y = eq.template proposal_sample<EXACT>(rng, overflow);
+    }
+    const V3<double> c{static_cast<double>(p.x), static_cast<double>(p.y), 0.0};
+    const double Rd = static_cast<double>(R);
+    const double distance = dist<DIM>(c, y);
+    if (!(distance > 0.0 && distance < Rd)) return 0.0;
+    const double green_mass = pg_mass_2d(Rd);
+    const double green_value = pg_green_2d(Rd, distance);
+    const double green_pdf = green_value / green_mass;
+    const double source_pdf = eq.proposal_pdf(y.x, y.y);
+    const double mixture_pdf = beta * green_pdf + (1.0 - beta) * source_pdf;
+    if (!(mixture_pdf > 0.0)) return 0.0;
+    const double source_value = eq.source(y);
+    return source_value == 0.0 ? 0.0 : green_value * source_value / mixture_pdf;
+}
+
 // One iteration of the walk loop body before the closest-point query
 // (include/wos/wos.hpp:69-115): the source contribution of the current ball,
 // the screening weight, then the step to the sphere.  Returns the new point.
@@ -575,7 +712,15 @@ __device__ __forceinline__ V3<T> walk_body(const Eq &eq, V3<T> p, T R, T &sample
     if constexpr (Eq::kSource) {
         bool may = true;
         if (DIM == 2) may = eq.may_intersect(p, R);
-        if (may) {
+        bool mis = false;
+        if constexpr (HasProposal<Eq>::value) {
+            if (may && eq.mode == kMis) {
+                sample += weight * static_cast<T>(
+                                       mis_contribution<DIM, EXACT, T>(eq, p, R, src, overflow));
+                mis = true;
+            }
+        }
+        if (may && !mis) {
             if (eq.mode == kGreen) {
                 const T radius = eq.green_radius(R, src, overflow);
                 const V3<T> sp = direction_at<DIM, EXACT, T>(p, radius, src);

@@ -21,6 +21,9 @@ struct FastRng {
     __device__ FastRng(uint64_t pseed, uint32_t walk) : s(pseed, walk) {}
     __device__ __forceinline__ T unit();
     __device__ __forceinline__ T unit_open() { return unit(); }
+    // (0, 1) with 53 random bits, for samplers that always work in double
+    __device__ __forceinline__ double unit64() { return s.uniform_d(); }
+    __device__ __forceinline__ double unit64_open() { return s.uniform_d(); }
 };
 template <>
 __device__ __forceinline__ float FastRng<float>::unit() { return s.uniform_f(); }

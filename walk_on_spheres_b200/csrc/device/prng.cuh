@@ -72,6 +72,10 @@ struct Xoshiro {
         for (int i = 0; i < 64 && v == 0.0; ++i) v = unit();
         return v;
     }
+
+    // FP64 draws for samplers that always work in double (same as above)
+    __device__ __forceinline__ double unit64() { return unit(); }
+    __device__ __forceinline__ double unit64_open() { return unit_open(); }
 };
 
 // Philox4x32-10 block function.

@@ -254,6 +254,12 @@ void launch_plain_dim(const SceneView &s, const PointSet &ps, uint64_t seed, EqD
                                       eps, max_steps, location, start, out, ctr, stream);
             }
             break;
+        case kPlate:
+            if (DIM == 2) {
+                launch_plain_typed<2>(s, ps, seed, Plate<2>{e.mode, *e.pl}, n_walks, eps,
+                                      max_steps, location, start, out, ctr, stream);
+            }
+            break;
         default:
             launch_plain_typed<DIM>(s, ps, seed, Helmholtz<DIM>{}, n_walks, eps, max_steps,
                                     location, start, out, ctr, stream);

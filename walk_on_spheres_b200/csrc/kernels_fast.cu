@@ -484,6 +484,8 @@ Helmholtz<2> eq_host(const EqDesc &) { return Helmholtz<2>{}; }
 template <>
 Transient<2> eq_host(const EqDesc &e) { return Transient<2>{kGreen, e.alpha, e.tr}; }
 template <>
+Plate<2> eq_host(const EqDesc &e) { return Plate<2>{e.mode, *e.pl}; }
+template <>
 Helmholtz<3> eq_host(const EqDesc &) { return Helmholtz<3>{}; }
 
 template <int DIM, class Eq>
@@ -544,6 +546,9 @@ cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const Fa
         case kTransient:
             return DIM == 2 ? launch_fast_typed<2, Transient<2>>(a, e, precision, plan, stream)
                             : cudaErrorInvalidValue;
+        case kPlate:
+            return DIM == 2 && e.pl ? launch_fast_typed<2, Plate<2>>(a, e, precision, plan, stream)
+                                    : cudaErrorInvalidValue;
         default:
             return launch_fast_typed<DIM, Helmholtz<DIM>>(a, e, precision, plan, stream);
     }
