@@ -113,7 +113,7 @@ int wos_batch::plan() {
         const BatchSolve &b = solves[s];
         const int dim = meshes[b.mesh]->scene.dim;
         const int prec = b.p.method == WOS_METHOD_FAST_FP32 ? 0 : 1;
-        const int hc = prec == 0 ? height_class(meshes[b.mesh]->dev.wide.H) + 1 : 0;
+        const int hc = prec == 0 ? traversal_class(meshes[b.mesh]->dev.wide) + 1 : 0;
         return ((dim * 8 + b.p.equation) * 2 + prec) * 8 + hc;
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
@@ -195,7 +195,7 @@ int wos_batch::plan() {
         it.max_ray_attempts = b.p.max_ray_attempts;
         it.precision = precision;
         it.point_begin = b.point_begin;
-        const int hc = precision == 32 ? height_class(m.dev.wide.H) : kHeightAny;
+        const int hc = precision == 32 ? traversal_class(m.dev.wide) : kHeightAny;
         if (families.empty() || families.back().dim != dim ||
             families.back().kind != b.p.equation || families.back().precision != precision ||
             families.back().hc != hc) {

@@ -81,12 +81,10 @@ __device__ __forceinline__ float wide_box_dist(const WideView &w, int h, int par
     return fmaxf(dx * dx + dy * dy + dz * dz, ds * ds);
 }
 
-// Primitive of this lane in leaf cluster `cluster`.
+// Squared distance to the primitive whose record starts at r (fields 32
+// floats apart).
 template <int DIM>
-__device__ __forceinline__ float wide_prim_dist(const WideView &w, int cluster, float px,
-                                                float py, float pz) {
-    constexpr int NF = DIM == 2 ? 5 : 16;
-    const float *r = w.prim + cluster * (NF * 32) + (threadIdx.x & 31u);
+__device__ __forceinline__ float prim_dist(const float *r, float px, float py, float pz) {
     if (DIM == 2) {
         const float x0 = r[0], y0 = r[32], vx = r[64], vy = r[96], inv = r[128];
         const float wx = px - x0, wy = py - y0;
@@ -101,19 +99,57 @@ __device__ __forceinline__ float wide_prim_dist(const WideView &w, int cluster, 
     return eberly32(px, py, pz, rec);
 }
 
-// Height classes of the traversal: a kernel compiled for one class carries
-// only that class's code (the other paths cost registers and instruction
-// cache on the hot ones).  kHeightAny keeps every path.
-enum : int { kHeightAny = -1, kHeightOther = 0, kHeightUpTo2 = 2, kHeight3 = 3 };
+// Primitive of this lane in leaf cluster `cluster`.
+template <int DIM>
+__device__ __forceinline__ float wide_prim_dist(const WideView &w, int cluster, float px,
+                                                float py, float pz) {
+    constexpr int NF = DIM == 2 ? 5 : 16;
+    return prim_dist<DIM>(w.prim + cluster * (NF * 32) + (threadIdx.x & 31u), px, py, pz);
+}
+
+// Closest primitive to (px, py, pz) found by one lane alone, testing every
+// primitive in slot order (the first minimum wins, as in wide_nearest).
+// For trees of at most kLanePrims primitives: a warp-cooperative query costs
+// about as much per query as one lane's whole scan there, and the lanes'
+// reads of one record are one broadcast.
+template <int DIM>
+__device__ __forceinline__ WideResult lane_nearest(const WideView &w, float px, float py,
+                                                   float pz) {
+    constexpr int NF = DIM == 2 ? 5 : 16;
+    float best = INFINITY;
+    int slot = -1;
+    for (int k = 0; k < w.n; ++k) {
+        const float d2 = prim_dist<DIM>(w.prim + (k >> 5) * (NF * 32) + (k & 31), px, py, pz);
+        if (d2 < best) {
+            best = d2;
+            slot = k;
+        }
+    }
+    return WideResult{best, slot};
+}
+
+// Traversal classes: a kernel compiled for one class carries only that
+// class's code (the other paths cost registers and instruction cache on the
+// hot ones).  kHeightAny keeps every path.  kLaneScan: at most kLanePrims
+// primitives, which the walk kernels scan lane by lane (lane_nearest);
+// wide_nearest treats it like kHeightUpTo2.
+enum : int { kHeightAny = -1, kHeightOther = 0, kLaneScan = 1, kHeightUpTo2 = 2, kHeight3 = 3 };
+
+__host__ __device__ __forceinline__ int lane_prims(int dim) { return dim == 2 ? 64 : 32; }
 
 __host__ __device__ __forceinline__ int height_class(int H) {
     return H <= 2 ? kHeightUpTo2 : (H == 3 ? kHeight3 : kHeightOther);
+}
+
+__host__ __device__ __forceinline__ int traversal_class(const WideView &w) {
+    return w.n <= lane_prims(w.dim) ? kLaneScan : height_class(w.H);
 }
 
 // Host dispatch: calls f(std::integral_constant<int, HC>{}) for class hc.
 template <class F>
 inline auto with_height_class(int hc, F &&f) {
     switch (hc) {
+        case kLaneScan: return f(std::integral_constant<int, kLaneScan>{});
         case kHeightUpTo2: return f(std::integral_constant<int, kHeightUpTo2>{});
         case kHeight3: return f(std::integral_constant<int, kHeight3>{});
         default: return f(std::integral_constant<int, kHeightOther>{});
@@ -146,7 +182,7 @@ __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, 
         m &= ~(1u << k);
         return k;
     };
-    if constexpr (HC == kHeightUpTo2 || HC == kHeightAny) {
+    if constexpr (HC == kHeightUpTo2 || HC == kLaneScan || HC == kHeightAny) {
     if (w.H == 1) {
         leaf(0);
         return WideResult{best, slot};

@@ -133,7 +133,17 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 }
             }
         }
-        if constexpr (kF32) {
+        if constexpr (kF32 && HC == kLaneScan) {
+            // a handful of primitives: every lane scans them for its own query
+            if (need_query) {
+                const WideResult q = lane_nearest<DIM>(wv, static_cast<float>(p.x),
+                                                       static_cast<float>(p.y),
+                                                       static_cast<float>(p.z));
+                const float r = sqrtf(q.best);
+                R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                slot = q.slot;
+            }
+        } else if constexpr (kF32) {
             // the warp resolves every pending closest-point query together
             unsigned pending = __ballot_sync(kFull, need_query);
             float qbest = 0.0f;
@@ -511,7 +521,7 @@ cudaError_t launch_fast_typed(const FastArgs &a, const EqDesc &e, int precision,
     };
     int blocks = 0;
     if (precision == 32) {
-        return with_height_class(height_class(a.w.H), [&](auto h) -> cudaError_t {
+        return with_height_class(traversal_class(a.w), [&](auto h) -> cudaError_t {
             constexpr int HC = decltype(h)::value;
             auto k = walk_fast_kernel<DIM, Eq, float, 3, HC>;
             if (plan.smem_bytes > 48 * 1024) {
