@@ -262,3 +262,41 @@ def test_wide_bvh_bounds_contain_primitives(mname):
                        dtype=np.float32) - np.float32(c))
             assert (t <= np.float32(th)).all(), (h, i, t.max(), th)
             assert abs(np.linalg.norm(nrm) - 1.0) < 1e-5
+
+
+def _tree_arrays(threads: int) -> dict:
+    """Binary and wide trees of a 57 120-triangle mesh built with `threads` host
+    threads (WOS_HOST_THREADS), in a fresh process."""
+    import json
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import json, sys, numpy as np, ctypes as C\n"
+        "sys.path.insert(0, %r)\n"
+        "from walk_on_spheres_b200 import meshes\n"
+        "from tests.test_host_abi import build_wide\n"
+        "from walk_on_spheres_b200 import _lib\n"
+        "m = meshes.perturbed_sphere(np.random.default_rng(11), 240, 120)\n"
+        "H, offs, nodes, order = build_wide(m)\n"
+        "L = _lib.lib(); vp = lambda a: a.ctypes.data_as(C.c_void_p)\n"
+        "v = np.ascontiguousarray(m.verts); p = np.ascontiguousarray(m.prims, dtype=np.int32)\n"
+        "D = C.c_int(); L.wos_build_bvh.restype = C.c_int\n"
+        "L.wos_build_bvh(3, vp(v), v.shape[0], vp(p), p.shape[0], 4, C.byref(D), None, None)\n"
+        "boxes = np.zeros((2 ** (D.value + 1)) * 6); border = np.zeros(p.shape[0], dtype=np.int32)\n"
+        "L.wos_build_bvh(3, vp(v), v.shape[0], vp(p), p.shape[0], 4, C.byref(D), vp(boxes), vp(border))\n"
+        "np.savez(sys.argv[1], H=H, offs=offs, nodes=nodes, order=order, boxes=boxes, border=border)\n"
+    ) % str(Path(__file__).resolve().parents[1])
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "t.npz")
+        env = dict(os.environ, WOS_HOST_THREADS=str(threads))
+        subprocess.run([sys.executable, "-c", code, out], check=True, env=env)
+        return dict(np.load(out))
+
+
+def test_threaded_build_is_bit_identical_to_a_serial_build():
+    serial, threaded = _tree_arrays(1), _tree_arrays(8)
+    assert serial["nodes"].size > 0 and serial["order"].size == 57120
+    for k in serial:
+        assert np.array_equal(serial[k], threaded[k]), k

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -11,15 +12,28 @@ namespace wosb {
 
 namespace {
 
+// Host threads of a build: WOS_HOST_THREADS when set to a positive count,
+// else the hardware's.
+unsigned host_threads() {
+    static const unsigned t = [] {
+        if (const char *e = std::getenv("WOS_HOST_THREADS")) {
+            const int v = std::atoi(e);
+            if (v >= 1) return static_cast<unsigned>(v);
+        }
+        return std::max(1u, std::thread::hardware_concurrency());
+    }();
+    return t;
+}
+
 // Subtree recursions split into host threads down to this depth (2^depth
 // threads at most); below it, or under kSerialItems items, they run inline.
 // Subtrees touch disjoint item ranges and node slots, so the result does not
 // depend on the thread count.
 int spawn_depth() {
     static const int d = [] {
-        unsigned hw = std::thread::hardware_concurrency();
+        const unsigned hw = host_threads();
         int k = 0;
-        while ((2u << k) <= std::max(1u, hw) && k < 6) ++k;
+        while ((2u << k) <= hw && k < 6) ++k;
         return k;
     }();
     return d;
@@ -41,7 +55,7 @@ void both(int depth, int items, F &&left, G &&right) {
 // Runs f(i) for i in [0, n) on the host threads, in contiguous blocks.
 template <class F>
 void parallel_for(long long n, F &&f) {
-    const long long threads = std::max(1u, std::thread::hardware_concurrency());
+    const long long threads = host_threads();
     if (n < 64 || threads == 1) {
         for (long long i = 0; i < n; ++i) f(i);
         return;
