@@ -427,6 +427,13 @@ int wos_prng_u64(wos_context *ctx, const uint64_t *seeds, long long n_seeds, int
 int wos_closest_points(wos_context *ctx, int precision, const double *points, long long n,
                        double *dist, double *nearest, int *boundary_id);
 
+/* ln I0(x) and ln K0(x) of the screened kernels as the walks evaluate them on
+ * the device (include/wos/bessel.hpp:16-87): precision 64 as PLAIN_FP64 /
+ * FAST_FP64 (series, quadrature and Hankel sums to FP64 accuracy), 32 as
+ * FAST_FP32 (x rounded to float; Abramowitz & Stegun 9.8.1-9.8.6). */
+int wos_special_functions(wos_context *ctx, int precision, const double *x, long long n,
+                          double *log_i0, double *log_k0);
+
 /* Scheduling overrides of the FAST methods (no reference counterpart):
  * walks per task and persistent grid size; <= 0 restores the automatic
  * choice.  Used by the benchmark's tuner. */

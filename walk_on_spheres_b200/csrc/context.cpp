@@ -526,6 +526,31 @@ extern "C" int wos_prng_u64(wos_context *ctx, const uint64_t *seeds, long long n
     return WOS_OK;
 }
 
+extern "C" int wos_special_functions(wos_context *ctx, int precision, const double *x,
+                                     long long n, double *log_i0, double *log_k0) {
+    if (!ctx || !x || !log_i0 || !log_k0 || n < 0 || (precision != 32 && precision != 64)) {
+        return fail(ctx, WOS_ERR_INVALID, "wos_special_functions: bad arguments");
+    }
+    cudaSetDevice(ctx->device);
+    const long long m = std::max<long long>(n, 1);
+    WOS_CUDA(ctx, ctx->scratch_a.reserve(sizeof(double) * m), "alloc");
+    WOS_CUDA(ctx, ctx->scratch_b.reserve(sizeof(double) * m), "alloc");
+    WOS_CUDA(ctx, ctx->scratch_c.reserve(sizeof(double) * m), "alloc");
+    WOS_CUDA(ctx, cudaMemcpyAsync(ctx->scratch_a.ptr, x, sizeof(double) * n,
+                                  cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    auto *di = static_cast<double *>(ctx->scratch_b.ptr);
+    auto *dk = static_cast<double *>(ctx->scratch_c.ptr);
+    WOS_CUDA(ctx, launch_special(precision, static_cast<const double *>(ctx->scratch_a.ptr), n,
+                                 di, dk, ctx->stream),
+             "special-function kernel");
+    WOS_CUDA(ctx, cudaMemcpyAsync(log_i0, di, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                  ctx->stream), "D2H");
+    WOS_CUDA(ctx, cudaMemcpyAsync(log_k0, dk, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                  ctx->stream), "D2H");
+    WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "special functions");
+    return WOS_OK;
+}
+
 extern "C" int wos_closest_points(wos_context *ctx, int precision, const double *points,
                                   long long n, double *dist, double *nearest, int *boundary_id) {
     if (!ctx || !ctx->has_mesh || !points || !dist || !nearest || n < 0 ||

@@ -122,6 +122,60 @@ __device__ __forceinline__ T log_k0(T x) {
     return -x + log(k0_scaled(x));
 }
 
+// FP32 walks (FAST_FP32): the polynomial approximations of Abramowitz &
+// Stegun, Handbook of Mathematical Functions, 9.8.1, 9.8.2, 9.8.5 and 9.8.6,
+// whose absolute errors on the scaled forms (I0(x) for x < 3.75,
+// sqrt(x) e^-x I0(x) above; K0(x) + ln(x/2) I0(x) for x <= 2, sqrt(x) e^x K0(x)
+// above) are below 1.9e-7.  That is FP32 resolution; the series and the
+// quadrature above would cost dozens of iterations per call for nothing.
+__device__ __forceinline__ float as_i0_small(float x) {  // 9.8.1, |x| < 3.75
+    const float t = x * (1.0f / 3.75f);
+    const float u = t * t;
+    return 1.0f +
+           u * (3.5156229f +
+                u * (3.0899424f +
+                     u * (1.2067492f + u * (0.2659732f + u * (0.0360768f + u * 0.0045813f)))));
+}
+
+template <>
+__device__ __forceinline__ float log_i0<float>(float x) {
+    x = fabsf(x);
+    if (x < 3.75f) return logf(as_i0_small(x));
+    const float u = 3.75f / x;  // 9.8.2
+    const float q =
+        0.39894228f +
+        u * (0.01328592f +
+             u * (0.00225319f +
+                  u * (-0.00157565f +
+                       u * (0.00916281f +
+                            u * (-0.02057706f +
+                                 u * (0.02635537f + u * (-0.01647633f + u * 0.00392377f)))))));
+    return x - 0.5f * logf(x) + logf(q);
+}
+
+template <>
+__device__ __forceinline__ float log_k0<float>(float x) {
+    if (x < 0.0f) return NAN;
+    if (x == 0.0f) return INFINITY;
+    if (x <= 2.0f) {  // 9.8.5
+        const float y = 0.25f * x * x;
+        const float k =
+            -logf(0.5f * x) * as_i0_small(x) +
+            (-0.57721566f +
+             y * (0.42278420f +
+                  y * (0.23069756f +
+                       y * (0.03488590f + y * (0.00262698f + y * (0.00010750f + y * 0.0000074f))))));
+        return logf(k);
+    }
+    const float u = 2.0f / x;  // 9.8.6
+    const float q =
+        1.25331414f +
+        u * (-0.07832358f +
+             u * (0.02189568f +
+                  u * (-0.01062446f + u * (0.00587872f + u * (-0.00251540f + u * 0.00053208f)))));
+    return -x - 0.5f * logf(x) + logf(q);
+}
+
 // include/wos/fastmath.hpp:15-28 (series truncated at a 1e-8 term)
 template <typename T>
 __device__ __forceinline__ T bessel_j0(T x) {

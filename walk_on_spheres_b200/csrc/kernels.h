@@ -166,6 +166,12 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
                         cudaStream_t stream, cudaEvent_t after_walk = nullptr);
 
 // Kernel-level checks.
+// ln I0(x) and ln K0(x) as the walk kernels of `precision` evaluate them
+// (64: the exact path's translation unit, 32: the fast path's).
+cudaError_t launch_special(int precision, const double *x, long long n, double *log_i0,
+                           double *log_k0, cudaStream_t stream);
+cudaError_t launch_special64(const double *x, long long n, double *log_i0, double *log_k0,
+                             cudaStream_t stream);
 cudaError_t launch_prng(const uint64_t *seeds, long long n, int count, uint64_t *out,
                         cudaStream_t stream);
 cudaError_t launch_closest64(const SceneView &s, const double *pts, long long n, double *dist,

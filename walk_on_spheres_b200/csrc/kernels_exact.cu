@@ -317,6 +317,22 @@ cudaError_t launch_walk_plain(const SceneView &s, const PointSet &ps, uint64_t s
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void special64_kernel(const double *x, long long n, double *li0, double *lk0) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    li0[i] = log_i0(x[i]);
+    lk0[i] = log_k0(x[i]);
+}
+}  // namespace
+
+cudaError_t launch_special64(const double *x, long long n, double *log_i0, double *log_k0,
+                             cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    special64_kernel<<<blocks_for(n, 128), 128, 0, stream>>>(x, n, log_i0, log_k0);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prng(const uint64_t *seeds, long long n, int count, uint64_t *out,
                         cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;

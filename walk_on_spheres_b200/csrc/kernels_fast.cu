@@ -566,6 +566,25 @@ cudaError_t launch_fast_dim(const FastArgs &a, EqDesc e, int precision, const Fa
 
 }  // namespace
 
+namespace {
+__global__ void special32_kernel(const double *x, long long n, double *li0, double *lk0) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float xf = static_cast<float>(x[i]);
+    li0[i] = static_cast<double>(log_i0(xf));
+    lk0[i] = static_cast<double>(log_k0(xf));
+}
+}  // namespace
+
+cudaError_t launch_special(int precision, const double *x, long long n, double *log_i0,
+                           double *log_k0, cudaStream_t stream) {
+    if (precision == 64) return launch_special64(x, n, log_i0, log_k0, stream);
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + 127) / 128;
+    special32_kernel<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(x, n, log_i0, log_k0);
+    return cudaGetLastError();
+}
+
 FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, int n_walks,
                    int precision, int device_sms, size_t smem_optin) {
     FastPlan p{};

@@ -194,6 +194,14 @@ class Solver:
                                                _ptr(near), _ptr(bid)))
         return dist, near, bid
 
+    def special_functions(self, x, precision: int = 64) -> tuple[np.ndarray, np.ndarray]:
+        """(ln I0(x), ln K0(x)) as the walk kernels of `precision` evaluate them."""
+        xs = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        li, lk = np.empty_like(xs), np.empty_like(xs)
+        self._check(self._L.wos_special_functions(self._ctx, precision, _ptr(xs), xs.size,
+                                                  _ptr(li), _ptr(lk)))
+        return li, lk
+
     def prng_u64(self, seeds, count: int) -> np.ndarray:
         s = np.ascontiguousarray(seeds, dtype=np.uint64)
         out = np.empty((s.shape[0], count), dtype=np.uint64)
