@@ -427,6 +427,16 @@ int wos_prng_u64(wos_context *ctx, const uint64_t *seeds, long long n_seeds, int
 int wos_closest_points(wos_context *ctx, int precision, const double *points, long long n,
                        double *dist, double *nearest, int *boundary_id);
 
+/* Lower bounds of the boundary distance that FAST_FP32 walks take from the
+ * mesh's distance lattice (no reference counterpart): FP64 distances at the
+ * nodes of a regular lattice over the bounding box, minus the distance to
+ * the nearest node, so bound <= the exact distance everywhere.  A walk step
+ * whose bound (times 1 - 2^-10) stays outside the epsilon shell uses it as
+ * its radius instead of a closest-point query; WoS is unbiased for any ball
+ * inside the domain.  NaN when the mesh has no lattice (meshes of at most 64
+ * segments or 32 triangles, or WOS_BOUND_GRID=0). */
+int wos_distance_bounds(wos_context *ctx, const double *points, long long n, double *bound);
+
 /* ln I0(x) and ln K0(x) of the screened kernels as the walks evaluate them on
  * the device (include/wos/bessel.hpp:16-87): precision 64 as PLAIN_FP64 /
  * FAST_FP64 (series, quadrature and Hankel sums to FP64 accuracy), 32 as

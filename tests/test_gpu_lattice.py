@@ -1,0 +1,35 @@
+"""The FAST_FP32 distance lattice (wos_distance_bounds): its bounds never
+exceed the exact FP64 boundary distance (so every lattice radius keeps the
+ball inside the domain) and are within half a lattice diagonal of it."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from walk_on_spheres_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mname,G", [("circle1024", 1024), ("annulus", 1024), ("sphere", 96),
+                                     ("star", 1024)])
+def test_bounds_are_valid_and_tight(solver, mname, G):
+    rng = np.random.default_rng(5)
+    m = {"circle1024": meshes.circle(segments=1024), "annulus": meshes.annulus(),
+         "sphere": meshes.uv_sphere(), "star": meshes.star_polygon(rng, 3000)}[mname]
+    solver.set_mesh(m)
+    lo, hi = np.asarray(solver.bbox[0::2][:m.dim]), np.asarray(solver.bbox[1::2][:m.dim])
+    pts = lo + (hi - lo) * rng.random((20000, m.dim))
+    bound = solver.distance_bounds(pts)
+    exact, _, _ = solver.closest_points(pts, precision=64)
+    assert np.all(np.isfinite(bound))
+    assert np.all(bound <= exact), np.max(bound - exact)
+    h = np.max(hi - lo) / (G - 1)
+    slack = h * np.sqrt(m.dim) * 1.0001 + 2e-6 * max(1.0, np.max(np.abs(hi)))
+    assert np.all(exact - bound <= slack), np.max(exact - bound) / slack
+
+
+def test_small_meshes_have_no_lattice(solver):
+    solver.set_mesh(meshes.circle(segments=32))
+    b = solver.distance_bounds(np.zeros((3, 2)))
+    assert np.all(np.isnan(b))

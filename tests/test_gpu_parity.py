@@ -111,9 +111,15 @@ def test_fast_statistically_equal(solver, oracle, case, method):
     assert abs(z.mean()) <= 4.0 / np.sqrt(max(1, z.size)), z.mean()
     # no standard error where the oracle has none (constant walks)
     assert np.all(np.abs(m_f[~live] - m_o[~live]) <= 1e-5 * np.maximum(1.0, np.abs(m_o[~live])))
-    # same walk-length distribution (mean steps within 5%)
+    # walk lengths: FAST_FP64 takes the oracle's balls (mean steps within 5%);
+    # FAST_FP32 may take lattice-bound balls, at least 1/2 of the upper bound
+    # of the distance, so its walks are longer, but never shorter
     st_o = ref.mean_steps.reshape(loc.shape)[ins].mean()
-    assert abs(res.mean_steps[ins].mean() / st_o - 1.0) <= 0.05
+    ratio = res.mean_steps[ins].mean() / st_o
+    if method == "fast64":
+        assert abs(ratio - 1.0) <= 0.05, ratio
+    else:
+        assert 0.95 <= ratio <= 1.6, ratio
 
 
 def test_solve_points_matches_grid(solver):

@@ -118,6 +118,7 @@ SIGNATURES = {
     "wos_prng_u64": (C.c_int, [VP, VP, C.c_longlong, C.c_int, VP]),
     "wos_closest_points": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP, VP]),
     "wos_special_functions": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP]),
+    "wos_distance_bounds": (C.c_int, [VP, VP, C.c_longlong, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
     "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
     "wos_transient_defaults": (None, [C.POINTER(TransientParams)]),

@@ -393,9 +393,7 @@ extern "C" int wos_batch_run(wos_batch *batch, int use_graph, float *device_ms) 
     WOS_CUDA(ctx, cudaStreamSynchronize(s), "batch run");
     for (const DeviceCounters &c : batch->host_counters) {
         if (c.error_flags) {
-            return fail(ctx, WOS_ERR_DEVICE,
-                        "a rejection sampler reached its proposal cap (error flags " +
-                            std::to_string(c.error_flags) + ")");
+            return fail(ctx, WOS_ERR_DEVICE, device_error(c.error_flags));
         }
     }
     if (device_ms) cudaEventElapsedTime(device_ms, batch->ev[0], batch->ev[1]);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -20,6 +21,16 @@ using namespace wosb;
 namespace {
 thread_local std::string g_error;
 }  // namespace
+
+std::string wosb::device_error(unsigned flags) {
+    std::string m;
+    if (flags & kErrRejectionCap) m = "a rejection sampler reached its proposal cap";
+    if (flags & kErrBadState) {
+        if (!m.empty()) m += "; ";
+        m += "a closest-point query found no boundary primitive";
+    }
+    return m + " (error flags " + std::to_string(flags) + ")";
+}
 
 int wosb::fail(wos_context *ctx, int code, const std::string &msg) {
     if (ctx) ctx->error = msg;
@@ -178,12 +189,61 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
     wide.box = static_cast<const float *>(wbox.ptr);
     wide.prim = static_cast<const float *>(wprim.ptr);
     wide.wide2bin = static_cast<const int *>(wide2bin.ptr);
+    return build_lattice(h, stream);
+}
+
+// The distance lattice of the FAST_FP32 walks (device/wide.cuh): nodes
+// spaced h = (largest bbox extent) / (G - 1) over the bounding box, G = 1024
+// in 2D and 96 in 3D (4 MB and 3.5 MB for a square / cubic box), FP64
+// distances from the binary tree.  Meshes of at most lane_prims primitives
+// query exactly at every step and get none; WOS_BOUND_GRID=0 turns it off.
+cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) {
+    wide.gd = nullptr;
+    if (h.n_prims <= lane_prims(h.dim)) return cudaSuccess;
+    if (const char *env = std::getenv("WOS_BOUND_GRID")) {
+        if (std::string(env) == "0") return cudaSuccess;
+    }
+    const int G = h.dim == 2 ? 1024 : 96;
+    double ext = 0.0, mag = 0.0;
+    for (int k = 0; k < h.dim; ++k) {
+        ext = std::max(ext, h.bbox[2 * k + 1] - h.bbox[2 * k]);
+        mag = std::max({mag, std::fabs(h.bbox[2 * k]), std::fabs(h.bbox[2 * k + 1])});
+    }
+    if (!(ext > 0.0)) return cudaSuccess;
+    const double step = ext / (G - 1);
+    int n[3] = {1, 1, 1};
+    double lo[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < h.dim; ++k) {
+        lo[k] = h.bbox[2 * k];
+        n[k] = static_cast<int>(std::ceil((h.bbox[2 * k + 1] - h.bbox[2 * k]) / step)) + 1;
+    }
+    // the device rebuilds node positions in FP32 (glo + i * gh): a few ulps
+    // of the largest coordinate, covered by the margin
+    const double margin = 1e-6 * std::max(mag, ext);
+    const size_t count = static_cast<size_t>(n[0]) * n[1] * n[2];
+    cudaError_t e = lattice.reserve(sizeof(float) * count);
+    if (e != cudaSuccess) return e;
+    auto *out = static_cast<float *>(lattice.ptr);
+    if ((e = launch_lattice(view, n, lo, step, margin, out, stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    wide.gd = out;
+    for (int k = 0; k < 3; ++k) {
+        wide.gn[k] = n[k];
+        wide.glo[k] = static_cast<float>(lo[k]);
+    }
+    wide.gh = static_cast<float>(step);
+    wide.ginv = static_cast<float>(1.0 / step);
+    wide.gratio = 3.0f;  // bound >= 1/2 of the upper bound
+    if (const char *env = std::getenv("WOS_LATTICE_RATIO")) {
+        const double r = std::atof(env);
+        if (r >= 1.0) wide.gratio = static_cast<float>(r);
+    }
     return cudaSuccess;
 }
 
 void SceneDevice::release() {
     for (DeviceBuffer *b : {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32,
-                            &wbox, &wprim, &wide2bin, &woff, &slotv}) {
+                            &wbox, &wprim, &wide2bin, &woff, &slotv, &lattice}) {
         b->release();
     }
 }
@@ -332,11 +392,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     WOS_CUDA(this, cudaMemcpyAsync(&hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, stream),
              "read counters");
     WOS_CUDA(this, cudaStreamSynchronize(stream), "solve");
-    if (hc.error_flags) {
-        return fail(this, WOS_ERR_DEVICE,
-                    "a rejection sampler reached its proposal cap (error flags " +
-                        std::to_string(hc.error_flags) + ")");
-    }
+    if (hc.error_flags) return fail(this, WOS_ERR_DEVICE, device_error(hc.error_flags));
     if (counters_out) {
         wos_counters &c = *counters_out;
         std::memset(&c, 0, sizeof(c));
@@ -548,6 +604,27 @@ extern "C" int wos_special_functions(wos_context *ctx, int precision, const doub
     WOS_CUDA(ctx, cudaMemcpyAsync(log_k0, dk, sizeof(double) * n, cudaMemcpyDeviceToHost,
                                   ctx->stream), "D2H");
     WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "special functions");
+    return WOS_OK;
+}
+
+extern "C" int wos_distance_bounds(wos_context *ctx, const double *points, long long n,
+                                   double *bound) {
+    if (!ctx || !ctx->has_mesh || !points || !bound || n < 0) {
+        return fail(ctx, WOS_ERR_INVALID, "wos_distance_bounds: bad arguments");
+    }
+    cudaSetDevice(ctx->device);
+    const int dim = ctx->scene.dim;
+    const long long m = std::max<long long>(n, 1);
+    WOS_CUDA(ctx, ctx->scratch_a.reserve(sizeof(double) * dim * m), "alloc");
+    WOS_CUDA(ctx, ctx->scratch_b.reserve(sizeof(double) * m), "alloc");
+    WOS_CUDA(ctx, cudaMemcpyAsync(ctx->scratch_a.ptr, points, sizeof(double) * dim * n,
+                                  cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    WOS_CUDA(ctx, launch_lattice_bounds(ctx->wide, static_cast<const double *>(ctx->scratch_a.ptr),
+                                        n, static_cast<double *>(ctx->scratch_b.ptr), ctx->stream),
+             "lattice kernel");
+    WOS_CUDA(ctx, cudaMemcpyAsync(bound, ctx->scratch_b.ptr, sizeof(double) * n,
+                                  cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "distance bounds");
     return WOS_OK;
 }
 

@@ -23,11 +23,13 @@ struct DeviceBuffer {
 // views the kernels take.
 struct SceneDevice {
     DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
-        wide2bin, woff, slotv;
+        wide2bin, woff, slotv, lattice;
     SceneView view{};
     WideView wide{};
     // Uploads `h` on `stream` (synchronised) and fills view / wide.
     cudaError_t upload(const HostScene &h, cudaStream_t stream);
+    // Builds the FAST_FP32 distance lattice into `lattice` and wide.gd.
+    cudaError_t build_lattice(const HostScene &h, cudaStream_t stream);
     void release();
 };
 
@@ -36,6 +38,9 @@ double effective_epsilon(const wos_params &p);
 // Frees a batch's device memory and detaches it from its context (called
 // for every live batch when the context is destroyed).
 void detach_batch(wos_batch *batch);
+
+// Message of a nonzero DeviceCounters::error_flags word.
+std::string device_error(unsigned flags);
 
 // Records `msg` as the context's (and the thread's) last error; returns code.
 int fail(wos_context *ctx, int code, const std::string &msg);

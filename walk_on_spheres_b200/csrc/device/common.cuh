@@ -76,6 +76,8 @@ struct DeviceCounters {
     unsigned int pad;
 };
 
+// error_flags bits: a bounded rejection loop ran out; a walk reached a state
+// the kernels must not act on (a closest-point query without a primitive)
 enum : unsigned { kErrRejectionCap = 1u, kErrBadState = 2u };
 
 // Output fields (any may be null).

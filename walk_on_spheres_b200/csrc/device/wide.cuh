@@ -40,7 +40,49 @@ struct WideView {
     const float *box;  // child-group blocks of (3*dim+2) x 32 floats
     const float *prim; // cluster blocks of 5 (2D) or 16 (3D) x 32 floats
     const int *wide2bin;
+    // Distance lattice (null when absent): gd[(i*gn[1] + j)*gn[2] + k] is a
+    // lower bound of the boundary distance at the node glo + (i, j, k) * gh
+    // as computed in FP32, so that d(x) >= gd[node] - |x - node| for every x
+    // (the distance function is 1-Lipschitz).
+    const float *gd;
+    int gn[3];
+    float glo[3];
+    float gh, ginv;
+    // a walk uses the lattice bound D - r (r = |x - node|) only when
+    // D >= gratio * r, i.e. when it is at least (gratio - 1) / (gratio + 1)
+    // of the upper bound D + r of the true distance
+    float gratio;
 };
+
+// Lattice value D at the node nearest to p and the distance r from p to it:
+// D - r <= d(p) <= D + r (up to D's downward rounding).
+struct LatticeSample {
+    float d, r;
+};
+
+template <int DIM>
+__device__ __forceinline__ LatticeSample lattice_sample(const WideView &w, float px, float py,
+                                                        float pz) {
+    const int i = min(max(__float2int_rn((px - w.glo[0]) * w.ginv), 0), w.gn[0] - 1);
+    const int j = min(max(__float2int_rn((py - w.glo[1]) * w.ginv), 0), w.gn[1] - 1);
+    const float dx = px - (w.glo[0] + static_cast<float>(i) * w.gh);
+    const float dy = py - (w.glo[1] + static_cast<float>(j) * w.gh);
+    if (DIM == 2) {
+        const float d = __ldg(w.gd + static_cast<long long>(i) * w.gn[1] + j);
+        return LatticeSample{d, sqrtf(dx * dx + dy * dy)};
+    }
+    const int k = min(max(__float2int_rn((pz - w.glo[2]) * w.ginv), 0), w.gn[2] - 1);
+    const float dz = pz - (w.glo[2] + static_cast<float>(k) * w.gh);
+    const float d = __ldg(w.gd + (static_cast<long long>(i) * w.gn[1] + j) * w.gn[2] + k);
+    return LatticeSample{d, sqrtf(dx * dx + dy * dy + dz * dz)};
+}
+
+// Lower bound of the boundary distance at p from the nearest lattice node.
+template <int DIM>
+__device__ __forceinline__ float lattice_bound(const WideView &w, float px, float py, float pz) {
+    const LatticeSample s = lattice_sample<DIM>(w, px, py, pz);
+    return s.d - s.r;
+}
 
 struct WideResult {
     float best;   // squared distance

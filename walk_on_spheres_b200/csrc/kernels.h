@@ -165,6 +165,15 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
                         unsigned long long *queue, HeatOut out, DeviceCounters *counters,
                         cudaStream_t stream, cudaEvent_t after_walk = nullptr);
 
+// Distance lattice of a scene: out[(i*n[1] + j)*n[2] + k] = the FP64
+// boundary distance at lo + (i, j, k) * h minus `margin`, rounded down to
+// float (0 if negative).
+cudaError_t launch_lattice(const SceneView &s, const int n[3], const double lo[3], double h,
+                           double margin, float *out, cudaStream_t stream);
+// lattice_bound at each point (FP32), NaN where the scene has no lattice.
+cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
+                                  cudaStream_t stream);
+
 // Kernel-level checks.
 // ln I0(x) and ln K0(x) as the walk kernels of `precision` evaluate them
 // (64: the exact path's translation unit, 32: the fast path's).

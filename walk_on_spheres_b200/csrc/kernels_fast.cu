@@ -55,6 +55,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     double mean_acc = 0.0, m2_acc = 0.0;
     unsigned hits = 0;
     bool overflow = false;
+    bool bad = false;  // a closest-point query found no primitive
 
     // per-lane walk state
     int walk = w0 + lane;
@@ -90,14 +91,20 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 bid = bid64;
             } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
                 // epsilon shell: FP64 re-projection onto the nearest primitive
-                const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
-                                                    static_cast<double>(p.x),
-                                                    static_cast<double>(p.y),
-                                                    static_cast<double>(p.z), np, bid);
-                if (d64 <= eps) {
+                // (a query that found none is a broken walk: flag it, stop)
+                if (slot < 0) {
+                    bad = true;
                     stop = true;
                 } else {
-                    R = static_cast<T>(d64);
+                    const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
+                                                        static_cast<double>(p.x),
+                                                        static_cast<double>(p.y),
+                                                        static_cast<double>(p.z), np, bid);
+                    if (d64 <= eps) {
+                        stop = true;
+                    } else {
+                        R = static_cast<T>(d64);
+                    }
                 }
             }
             if (!stop && steps >= a.max_steps) {
@@ -106,9 +113,13 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 ++hits;
                 stop = true;
                 if (kF32) {
-                    reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
-                                     static_cast<double>(p.y), static_cast<double>(p.z), np,
-                                     bid);
+                    if (slot < 0) {
+                        bad = true;
+                    } else {
+                        reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
+                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
+                                         bid);
+                    }
                 } else {
                     np = np64;
                     bid = bid64;
@@ -123,6 +134,20 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 ++steps;
                 if constexpr (kF32) {
                     need_query = true;
+                    if constexpr (HC != kLaneScan) {
+                        // away from the shell a lattice lower bound is a valid
+                        // (smaller) radius and spares the exact query; the step
+                        // that reaches the cap queries, for its nearest point
+                        if (wv.gd != nullptr && steps < a.max_steps) {
+                            const LatticeSample ls =
+                                lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
+                            const float gb = (ls.d - ls.r) * a.shrink;
+                            if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
+                                R = gb;
+                                need_query = false;
+                            }
+                        }
+                    }
                 } else {
                     const Nearest<double> q = nearest64<DIM>(
                         a.s, static_cast<double>(p.x), static_cast<double>(p.y),
@@ -207,7 +232,9 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         hits += hb;
     }
     const unsigned any_overflow = __ballot_sync(kFull, overflow);
+    const unsigned any_bad = __ballot_sync(kFull, bad);
     if (lane == 0) {
+        if (any_bad) atomicOr(&a.ctr->error_flags, kErrBadState);
         TaskPartial tp;
         tp.n = n_tot;
         tp.mean = mean_acc;
@@ -575,6 +602,34 @@ __global__ void special32_kernel(const double *x, long long n, double *li0, doub
     lk0[i] = static_cast<double>(log_k0(xf));
 }
 }  // namespace
+
+namespace {
+template <int DIM>
+__global__ void lattice_bounds_kernel(WideView w, const double *pts, long long n, double *out) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (w.gd == nullptr) {
+        out[i] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const float px = static_cast<float>(pts[DIM * i]);
+    const float py = static_cast<float>(pts[DIM * i + 1]);
+    const float pz = DIM == 3 ? static_cast<float>(pts[DIM * i + 2]) : 0.0f;
+    out[i] = static_cast<double>(lattice_bound<DIM>(w, px, py, pz));
+}
+}  // namespace
+
+cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
+                                  cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((n + 127) / 128);
+    if (w.dim == 2) {
+        lattice_bounds_kernel<2><<<blocks, 128, 0, stream>>>(w, pts, n, out);
+    } else {
+        lattice_bounds_kernel<3><<<blocks, 128, 0, stream>>>(w, pts, n, out);
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_special(int precision, const double *x, long long n, double *log_i0,
                            double *log_k0, cudaStream_t stream) {

@@ -173,9 +173,7 @@ extern "C" int wos_solve_grid_device_noalloc(wos_context *ctx, const wos_params 
     e = cudaMemcpyAsync(&hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(ctx, WOS_ERR_CUDA, std::string("solve: ") + cudaGetErrorString(e));
-    if (hc.error_flags) {
-        return fail(ctx, WOS_ERR_DEVICE, "a rejection sampler reached its proposal cap");
-    }
+    if (hc.error_flags) return fail(ctx, WOS_ERR_DEVICE, wosb::device_error(hc.error_flags));
     if (counters) {
         std::memset(counters, 0, sizeof(*counters));
         counters->max_steps_hits = static_cast<long long>(hc.max_steps_hits);

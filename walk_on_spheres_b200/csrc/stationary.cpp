@@ -233,11 +233,12 @@ extern "C" int wos_stationary_solve(wos_context *ctx, const wos_stationary_param
 
     DeviceCounters hc[2];
     WOS_CUDA(ctx, cudaMemcpy(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost), "read counters");
-    if (hc[0].error_flags) {
+    if (hc[0].error_flags == kErrRejectionCap) {
         // gaussian_heat_source.hpp:70-72
         return fail(ctx, WOS_ERR_DEVICE,
                     "finite-plate Gaussian rejection sampler did not accept a point");
     }
+    if (hc[0].error_flags) return fail(ctx, WOS_ERR_DEVICE, device_error(hc[0].error_flags));
     if (max_steps_hits) *max_steps_hits = static_cast<long long>(hc[0].max_steps_hits);
     double *dst[4] = {mean, variance, standard_error, mean_steps};
     for (int k = 0; k < 4; ++k) {

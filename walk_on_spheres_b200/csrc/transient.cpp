@@ -347,9 +347,7 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
     long long hits = 0;
     for (const DeviceCounters &c : hc) {
         if (c.error_flags) {
-            return fail(ctx, WOS_ERR_DEVICE,
-                        "a rejection sampler reached its proposal cap (error flags " +
-                            std::to_string(c.error_flags) + ")");
+            return fail(ctx, WOS_ERR_DEVICE, device_error(c.error_flags));
         }
         hits += static_cast<long long>(c.max_steps_hits);
     }

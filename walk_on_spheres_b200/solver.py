@@ -194,6 +194,13 @@ class Solver:
                                                _ptr(near), _ptr(bid)))
         return dist, near, bid
 
+    def distance_bounds(self, points) -> np.ndarray:
+        """Lattice lower bounds of the boundary distance used by FAST_FP32 walks."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, self.dim)
+        out = np.empty(pts.shape[0])
+        self._check(self._L.wos_distance_bounds(self._ctx, _ptr(pts), pts.shape[0], _ptr(out)))
+        return out
+
     def special_functions(self, x, precision: int = 64) -> tuple[np.ndarray, np.ndarray]:
         """(ln I0(x), ln K0(x)) as the walk kernels of `precision` evaluate them."""
         xs = np.ascontiguousarray(x, dtype=np.float64).ravel()
