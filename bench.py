@@ -65,8 +65,8 @@ UNIT = "walks/s"
 BYTES_PER_QUERY = 1863.4
 # DRAM bytes (read + write) of one walk-kernel launch of this workload, from a
 # one-pass ncu capture of the full launch (profiles/walk_fast_kernel_poisson2d_
-# circle1024.md): 2.84 MB and 3.32 MB for the two source modes.
-TRAFFIC_BYTES_PER_LAUNCH = 3.08e6
+# circle1024.md): 6.21 MB and 6.25 MB for the two source modes.
+TRAFFIC_BYTES_PER_LAUNCH = 6.23e6
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
 # 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in
 # the interior, 2048 FP32 walks each; one "gradient" is one full backward
@@ -446,7 +446,11 @@ def gpu_arm(args, rank, world, local):
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
                      "algorithmic_bytes": f"{BYTES_PER_QUERY} B per closest-point query x "
-                                          f"{queries_per_launch:.0f} queries per launch"},
+                                          f"{queries_per_launch:.0f} queries per launch",
+                     "note": "algorithmic bytes of the reference traversal per walk step; "
+                             "the mesh is staged in shared memory and most steps take "
+                             "their radius from the L2-resident distance lattice, so the "
+                             "kernel is issue-bound and frac > 1 is expected"},
         "clocks": clock,
         "wall_s_timed_region": wall,
     }
