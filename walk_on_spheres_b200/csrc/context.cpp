@@ -194,16 +194,17 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
 
 // The distance lattice of the FAST_FP32 walks (device/wide.cuh): nodes
 // spaced h = (largest bbox extent) / (G - 1) over the bounding box, G = 1024
-// in 2D and 96 in 3D (4 MB and 3.5 MB for a square / cubic box), FP64
-// distances from the binary tree.  Meshes of at most lane_prims primitives
-// query exactly at every step and get none; WOS_BOUND_GRID=0 turns it off.
+// in 2D and 160 in 3D (4 MB and 16 MB for a square / cubic box), distances
+// from the exact FP32 cooperative query at the nodes' FP32 positions.
+// Meshes of at most lane_prims primitives query exactly at every step and get
+// none; WOS_BOUND_GRID=0 turns it off.
 cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) {
     wide.gd = nullptr;
     if (h.n_prims <= lane_prims(h.dim)) return cudaSuccess;
     if (const char *env = std::getenv("WOS_BOUND_GRID")) {
         if (std::string(env) == "0") return cudaSuccess;
     }
-    const int G = h.dim == 2 ? 1024 : 96;
+    const int G = h.dim == 2 ? 1024 : 160;
     double ext = 0.0, mag = 0.0;
     for (int k = 0; k < h.dim; ++k) {
         ext = std::max(ext, h.bbox[2 * k + 1] - h.bbox[2 * k]);
@@ -212,28 +213,29 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
     if (!(ext > 0.0)) return cudaSuccess;
     const double step = ext / (G - 1);
     int n[3] = {1, 1, 1};
-    double lo[3] = {0.0, 0.0, 0.0};
     for (int k = 0; k < h.dim; ++k) {
-        lo[k] = h.bbox[2 * k];
         n[k] = static_cast<int>(std::ceil((h.bbox[2 * k + 1] - h.bbox[2 * k]) / step)) + 1;
+        wide.glo[k] = static_cast<float>(h.bbox[2 * k]);
     }
-    // the device rebuilds node positions in FP32 (glo + i * gh): a few ulps
-    // of the largest coordinate, covered by the margin
-    const double margin = 1e-6 * std::max(mag, ext);
+    for (int k = 0; k < 3; ++k) wide.gn[k] = n[k];
+    if (h.dim == 2) wide.glo[2] = 0.0f;
+    wide.gh = static_cast<float>(step);
+    wide.ginv = static_cast<float>(1.0 / step);
+    // FP32 primitive distances carry a few ulps of the largest coordinate
+    const float margin = static_cast<float>(4e-6 * std::max(mag, ext));
     const size_t count = static_cast<size_t>(n[0]) * n[1] * n[2];
     cudaError_t e = lattice.reserve(sizeof(float) * count);
     if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) {
+        return e;
+    }
     auto *out = static_cast<float *>(lattice.ptr);
-    if ((e = launch_lattice(view, n, lo, step, margin, out, stream)) != cudaSuccess) return e;
+    if ((e = launch_lattice32(wide, margin, out, sms, stream)) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     wide.gd = out;
-    for (int k = 0; k < 3; ++k) {
-        wide.gn[k] = n[k];
-        wide.glo[k] = static_cast<float>(lo[k]);
-    }
-    wide.gh = static_cast<float>(step);
-    wide.ginv = static_cast<float>(1.0 / step);
-    wide.gratio = 3.0f;  // bound >= 1/2 of the upper bound
+    wide.gratio = 2.0f;  // bound >= 1/3 of the upper bound
     if (const char *env = std::getenv("WOS_LATTICE_RATIO")) {
         const double r = std::atof(env);
         if (r >= 1.0) wide.gratio = static_cast<float>(r);

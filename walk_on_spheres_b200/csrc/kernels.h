@@ -165,11 +165,13 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
                         unsigned long long *queue, HeatOut out, DeviceCounters *counters,
                         cudaStream_t stream, cudaEvent_t after_walk = nullptr);
 
-// Distance lattice of a scene: out[(i*n[1] + j)*n[2] + k] = the FP64
-// boundary distance at lo + (i, j, k) * h minus `margin`, rounded down to
-// float (0 if negative).
-cudaError_t launch_lattice(const SceneView &s, const int n[3], const double lo[3], double h,
-                           double margin, float *out, cudaStream_t stream);
+// Distance lattice of a scene (w's lattice geometry gn / glo / gh set, gd
+// unused): out[(i*gn[1] + j)*gn[2] + k] = the exact FP32 cooperative query's
+// boundary distance at the FP32 node glo + (i, j, k) * gh, minus `margin`,
+// rounded down (0 if negative).  FP64 per-thread queries took 240 ms for a
+// 173k-triangle mesh at 160^3 nodes.
+cudaError_t launch_lattice32(const WideView &w, float margin, float *out, int sms,
+                            cudaStream_t stream);
 // lattice_bound at each point (FP32), NaN where the scene has no lattice.
 cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
                                   cudaStream_t stream);

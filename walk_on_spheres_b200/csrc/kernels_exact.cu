@@ -319,27 +319,6 @@ cudaError_t launch_walk_plain(const SceneView &s, const PointSet &ps, uint64_t s
 }
 
 namespace {
-template <int DIM>
-__global__ void lattice_kernel(SceneView s, int nx, int ny, int nz, double lox, double loy,
-                               double loz, double h, double margin, float *out) {
-    const long long n = static_cast<long long>(nx) * ny * nz;
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
-         t += stride) {
-        const int k = static_cast<int>(t % nz);
-        const long long r = t / nz;
-        const int j = static_cast<int>(r % ny);
-        const int i = static_cast<int>(r / ny);
-        const double x = lox + static_cast<double>(i) * h;
-        const double y = loy + static_cast<double>(j) * h;
-        const double z = DIM == 3 ? loz + static_cast<double>(k) * h : 0.0;
-        const Nearest<double> q =
-            nearest64<DIM>(s, x, y, z, __longlong_as_double(0x7ff0000000000000LL));
-        const double d = sqrt(q.best) - margin;
-        out[t] = d > 0.0 ? __double2float_rd(d) : 0.0f;
-    }
-}
-
 __global__ void special64_kernel(const double *x, long long n, double *li0, double *lk0) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -347,21 +326,6 @@ __global__ void special64_kernel(const double *x, long long n, double *li0, doub
     lk0[i] = log_k0(x[i]);
 }
 }  // namespace
-
-cudaError_t launch_lattice(const SceneView &s, const int n[3], const double lo[3], double h,
-                           double margin, float *out, cudaStream_t stream) {
-    const long long total = static_cast<long long>(n[0]) * n[1] * n[2];
-    if (total <= 0) return cudaSuccess;
-    const long long b = std::min<long long>((total + 127) / 128, 148 * 16);
-    if (s.dim == 2) {
-        lattice_kernel<2><<<static_cast<int>(b), 128, 0, stream>>>(s, n[0], n[1], n[2], lo[0],
-                                                                   lo[1], lo[2], h, margin, out);
-    } else {
-        lattice_kernel<3><<<static_cast<int>(b), 128, 0, stream>>>(s, n[0], n[1], n[2], lo[0],
-                                                                   lo[1], lo[2], h, margin, out);
-    }
-    return cudaGetLastError();
-}
 
 cudaError_t launch_special64(const double *x, long long n, double *log_i0, double *log_k0,
                              cudaStream_t stream) {

@@ -550,7 +550,10 @@ cudaError_t launch_fast_typed(const FastArgs &a, const EqDesc &e, int precision,
     if (precision == 32) {
         return with_height_class(traversal_class(a.w), [&](auto h) -> cudaError_t {
             constexpr int HC = decltype(h)::value;
-            auto k = walk_fast_kernel<DIM, Eq, float, 3, HC>;
+            // 4 blocks / SM (64 registers) for the height <= 3 traversals,
+            // 3 for the generic one
+            constexpr int kMinBlocks = (HC == kHeightUpTo2 || HC == kHeight3) ? 4 : 3;
+            auto k = walk_fast_kernel<DIM, Eq, float, kMinBlocks, HC>;
             if (plan.smem_bytes > 48 * 1024) {
                 cudaError_t err = cudaFuncSetAttribute(
                     k, cudaFuncAttributeMaxDynamicSharedMemorySize, plan.smem_bytes);
@@ -604,6 +607,33 @@ __global__ void special32_kernel(const double *x, long long n, double *li0, doub
 }  // namespace
 
 namespace {
+// One lattice node per warp: the exact (keep = 1) FP32 cooperative query at
+// the node's FP32 position glo + (i, j, k) gh, the same position the walks'
+// lattice_sample rebuilds.  `margin` covers the FP32 rounding of the
+// primitive distances (a few ulps of the coordinates); sqrtf is correctly
+// rounded and the factor below takes it down.
+template <int DIM>
+__global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin, float *out) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    for (long long t = warp; t < n; t += warps) {
+        const int k = static_cast<int>(t % w.gn[2]);
+        const long long r = t / w.gn[2];
+        const int j = static_cast<int>(r % w.gn[1]);
+        const int i = static_cast<int>(r / w.gn[1]);
+        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+        const float y = w.glo[1] + static_cast<float>(j) * w.gh;
+        const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
+        const WideResult q = wide_nearest<DIM>(w, x, y, z, 1.0f, 0.0f);
+        if (lane == 0) {
+            const float d = (sqrtf(q.best) - margin) * (1.0f - 0x1p-20f);
+            out[t] = d > 0.0f ? d : 0.0f;
+        }
+    }
+}
+
 template <int DIM>
 __global__ void lattice_bounds_kernel(WideView w, const double *pts, long long n, double *out) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -618,6 +648,19 @@ __global__ void lattice_bounds_kernel(WideView w, const double *pts, long long n
     out[i] = static_cast<double>(lattice_bound<DIM>(w, px, py, pz));
 }
 }  // namespace
+
+cudaError_t launch_lattice32(const WideView &w, float margin, float *out, int sms,
+                            cudaStream_t stream) {
+    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
+    if (w.dim == 2) {
+        lattice32_kernel<2><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+    } else {
+        lattice32_kernel<3><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
                                   cudaStream_t stream) {
