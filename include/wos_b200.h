@@ -209,7 +209,10 @@ typedef struct wos_batch wos_batch;
 int wos_batch_create(wos_context *ctx, wos_batch **out);
 void wos_batch_destroy(wos_batch *batch);
 
-/* Add a mesh (arguments as wos_set_mesh); *mesh_id indexes it. */
+/* Add a mesh (arguments as wos_set_mesh); *mesh_id indexes it.  The mesh is
+ * checked now (wos_set_mesh's errors and messages); its trees are built with
+ * the batch's other new meshes, in parallel on the host threads, by
+ * wos_batch_prepare or the next wos_batch_run. */
 int wos_batch_add_mesh(wos_batch *batch, int dim, const double *verts, int n_verts,
                        const int *prims, int n_prims, const int *boundary_ids, int leaf_size,
                        int *mesh_id);
@@ -222,6 +225,11 @@ int wos_batch_add_solve(wos_batch *batch, int mesh_id, const wos_params *params,
 /* Walks per task (<= 0: min(N_walks, 1024) per solve) and persistent grid
  * size of every walk launch (<= 0: every block that can be resident). */
 int wos_batch_set_tuning(wos_batch *batch, int chunk, int blocks);
+
+/* Build and upload the meshes added since the last run and lay out every
+ * solve (what the first wos_batch_run does before launching), so that set-up
+ * can be timed or overlapped apart from the runs. */
+int wos_batch_prepare(wos_batch *batch);
 
 /* Run every solve.  use_graph != 0 captures the launch sequence as a CUDA
  * graph on the first run (and after any change to the batch) and replays

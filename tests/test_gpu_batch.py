@@ -3,7 +3,7 @@ same solve run alone through wos_solve_grid, with and without CUDA-graph
 capture: identical locations, counters and per-point step counts (the walks
 are the same), statistics equal to 1e-12 relative (the batch kernel may
 round the terminal FP64 arithmetic differently); graph replays are
-bit-for-bit deterministic; invalid solves are rejected."""
+bit-for-bit deterministic; invalid solves and meshes are rejected."""
 from __future__ import annotations
 
 import numpy as np
@@ -126,6 +126,20 @@ def test_batch_rejects_invalid_solves(solver):
         b.add_solve(m + 1, "laplace", 8, 8, N_walks=10, method="fast")
     with pytest.raises(WosError, match="alpha"):
         b.add_solve(m, "screened_poisson", 8, 8, N_walks=10, alpha=0.0, method="fast")
+    # meshes are checked when added, with wos_set_mesh's messages
+    from walk_on_spheres_b200.meshes import Mesh
+    bad = Mesh(2, np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 0.0]]),
+               np.array([[0, 1], [1, 2], [2, 0]], dtype=np.int32), np.zeros(3, dtype=np.int32))
+    with pytest.raises(WosError, match="zero-length line segment"):
+        b.add_mesh(bad)
+    # prepare() builds the new meshes (in parallel) before the first run; the
+    # solve then matches the same solve alone
+    sid = b.add_solve(m, "laplace", 9, 9, N_walks=64, seed=3, method="fast")
+    b.prepare()
+    b.run(use_graph=False)
+    solver.set_mesh(meshes.annulus())
+    _assert_reproduces(b.result(sid), solver.solve_grid("laplace", 9, 9, N_walks=64, seed=3,
+                                                        method="fast"))
     # an empty batch runs
     b2 = Batch(solver)
     b2.run(use_graph=True)

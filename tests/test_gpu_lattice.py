@@ -25,8 +25,10 @@ def test_bounds_are_valid_and_tight(solver, mname, G):
     assert np.all(np.isfinite(bound))
     assert np.all(bound <= exact), np.max(bound - exact)
     h = np.max(hi - lo) / (G - 1)
-    slack = h * np.sqrt(m.dim) * 1.0001 + 1e-5 * max(1.0, np.max(np.abs(hi)))
-    assert np.all(exact - bound <= slack), np.max(exact - bound) / slack
+    # node values are the conservatively pruned query: within 1 - 2^-10 of
+    # the node distance
+    slack = h * np.sqrt(m.dim) * 1.0001 + 2.0 ** -10 * exact + 1e-5 * max(1.0, np.max(np.abs(hi)))
+    assert np.all(exact - bound <= slack), np.max((exact - bound) / slack)
 
 
 def test_small_meshes_have_no_lattice(solver):

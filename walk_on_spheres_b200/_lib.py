@@ -135,6 +135,7 @@ SIGNATURES = {
     "wos_batch_add_solve": (C.c_int, [VP, C.c_int, C.POINTER(Params), C.POINTER(Grid),
                                       C.POINTER(C.c_int)]),
     "wos_batch_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_batch_prepare": (C.c_int, [VP]),
     "wos_batch_run": (C.c_int, [VP, C.c_int, C.POINTER(C.c_float)]),
     "wos_batch_info": (C.c_int, [VP, C.POINTER(C.c_int)] + [C.POINTER(C.c_longlong)] * 3),
     "wos_batch_result": (C.c_int, [VP, C.c_int] + [VP] * 5 + [C.POINTER(Counters)]),

@@ -76,6 +76,10 @@ class Batch:
     def set_tuning(self, chunk: int = 0, blocks: int = 0):
         self.solver._check(self._L.wos_batch_set_tuning(self._b, int(chunk), int(blocks)))
 
+    def prepare(self) -> None:
+        """Build and upload new meshes and lay out the solves (else the next run does)."""
+        self.solver._check(self._L.wos_batch_prepare(self._b))
+
     def run(self, use_graph: bool = True) -> float:
         ms = C.c_float()
         self.solver._check(self._L.wos_batch_run(self._b, int(bool(use_graph)), C.byref(ms)))

@@ -11,11 +11,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/wos_b200.h"
@@ -26,7 +28,14 @@ using namespace wosb;
 
 namespace {
 
+// A mesh is checked when it is added and built later, with the batch's
+// other pending meshes, in parallel (wos_batch::prepare).
 struct BatchMesh {
+    int dim = 0;
+    int leaf_size = 0;
+    std::vector<double> verts;   // inputs until built
+    std::vector<int> prims, bids;
+    bool built = false;
     HostScene scene;
     SceneDevice dev;
 };
@@ -100,11 +109,53 @@ struct wos_batch {
         drop_graph();
     }
 
+    int prepare();
     int plan();
     cudaError_t enqueue();
 };
 
+// Builds every pending mesh's trees on the host threads (one mesh per
+// thread, each build itself threaded for large meshes), then uploads them
+// and builds their lattices on the context's stream.
+int wos_batch::prepare() {
+    std::vector<BatchMesh *> todo;
+    for (auto &m : meshes) {
+        if (!m->built) todo.push_back(m.get());
+    }
+    if (todo.empty()) return WOS_OK;
+    std::vector<std::string> errs(todo.size());
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i = next++; i < todo.size(); i = next++) {
+            BatchMesh &m = *todo[i];
+            errs[i] = build_scene(m.dim, m.verts.data(), static_cast<int>(m.verts.size()) / m.dim,
+                                  m.prims.data(), static_cast<int>(m.prims.size()) / m.dim,
+                                  m.bids.empty() ? nullptr : m.bids.data(), m.leaf_size, m.scene);
+        }
+    };
+    const size_t workers = std::min<size_t>(todo.size(), host_threads());
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < workers; ++t) pool.emplace_back(work);
+    work();
+    for (std::thread &t : pool) t.join();
+    cudaSetDevice(ctx->device);
+    for (size_t i = 0; i < todo.size(); ++i) {
+        if (!errs[i].empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + errs[i]);
+        BatchMesh &m = *todo[i];
+        WOS_CUDA(ctx, m.dev.upload(m.scene, ctx->stream), "batch mesh upload");
+        m.built = true;
+        m.verts.clear();
+        m.verts.shrink_to_fit();
+        m.prims.clear();
+        m.prims.shrink_to_fit();
+        m.bids.clear();
+        m.bids.shrink_to_fit();
+    }
+    return WOS_OK;
+}
+
 int wos_batch::plan() {
+    if (const int rc = prepare()) return rc;
     cudaSetDevice(ctx->device);
     const int n = static_cast<int>(solves.size());
     order.resize(n);
@@ -295,11 +346,14 @@ extern "C" int wos_batch_add_mesh(wos_batch *batch, int dim, const double *verts
                                   int leaf_size, int *mesh_id) {
     if (const int rc = batch_ok(batch, "wos_batch_add_mesh")) return rc;
     wos_context *ctx = batch->ctx;
-    auto m = std::make_unique<BatchMesh>();
-    const std::string err =
-        build_scene(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, m->scene);
+    const std::string err = check_mesh(dim, verts, n_verts, prims, n_prims, leaf_size);
     if (!err.empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + err);
-    WOS_CUDA(ctx, m->dev.upload(m->scene, ctx->stream), "batch mesh upload");
+    auto m = std::make_unique<BatchMesh>();
+    m->dim = dim;
+    m->leaf_size = leaf_size;
+    m->verts.assign(verts, verts + static_cast<size_t>(n_verts) * dim);
+    m->prims.assign(prims, prims + static_cast<size_t>(n_prims) * dim);
+    if (dim == 2 && boundary_ids) m->bids.assign(boundary_ids, boundary_ids + n_prims);
     batch->meshes.push_back(std::move(m));
     if (mesh_id) *mesh_id = static_cast<int>(batch->meshes.size()) - 1;
     batch->invalidate();
@@ -323,7 +377,7 @@ extern "C" int wos_batch_add_solve(wos_batch *batch, int mesh_id, const wos_para
         err = "alpha must be positive";
     else if (p->method != WOS_METHOD_FAST_FP32 && p->method != WOS_METHOD_FAST_FP64)
         err = "batches run FAST_FP32 or FAST_FP64";
-    const int dim = err.empty() ? batch->meshes[mesh_id]->scene.dim : 2;
+    const int dim = err.empty() ? batch->meshes[mesh_id]->dim : 2;
     if (err.empty() && (g->Nx < 1 || g->Ny < 1 || (dim == 3 && g->Nz < 1))) {
         err = "grid sizes must be >= 1";
     }
@@ -350,6 +404,12 @@ extern "C" int wos_batch_set_tuning(wos_batch *batch, int chunk, int blocks) {
     batch->blocks_override = blocks;
     batch->invalidate();
     return WOS_OK;
+}
+
+extern "C" int wos_batch_prepare(wos_batch *batch) {
+    if (const int rc = batch_ok(batch, "wos_batch_prepare")) return rc;
+    if (batch->planned) return WOS_OK;
+    return batch->plan();
 }
 
 extern "C" int wos_batch_run(wos_batch *batch, int use_graph, float *device_ms) {

@@ -63,15 +63,6 @@ cudaError_t DeviceBuffer::reserve(size_t n) {
     return cudaSuccess;
 }
 
-template <typename T>
-static cudaError_t upload(DeviceBuffer &b, const std::vector<T> &v, cudaStream_t s) {
-    const size_t n = std::max<size_t>(v.size() * sizeof(T), 16);
-    cudaError_t e = b.reserve(n);
-    if (e != cudaSuccess) return e;
-    if (v.empty()) return cudaMemsetAsync(b.ptr, 0, n, s);
-    return cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-}
-
 wos_context::~wos_context() {
     for (DeviceBuffer *b : all_buffers()) b->release();
     sdev.release();
@@ -148,47 +139,69 @@ extern "C" void wos_context_destroy(wos_context *ctx) {
 
 // ------------------------------------------------------------- mesh
 
+// One device allocation per scene (arrays at 256-byte aligned offsets): a
+// set_mesh or batch mesh costs one cudaMalloc instead of one per array.
 cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
-    cudaError_t e;
-#define WOS_UP(buf, vec) \
-    if ((e = ::upload(buf, vec, stream)) != cudaSuccess) return e
-    WOS_UP(box64, h.box64);
-    WOS_UP(seg64, h.seg64);
-    WOS_UP(segid, h.segid);
-    WOS_UP(tri64, h.tri64);
-    WOS_UP(pair32, h.pair32);
-    WOS_UP(seg32, h.seg32);
-    WOS_UP(seg32inv, h.seg32inv);
-    WOS_UP(tri32, h.tri32);
-    WOS_UP(wbox, h.wbox);
-    WOS_UP(wprim, h.wprim);
-    WOS_UP(wide2bin, h.wide2bin);
-    WOS_UP(woff, std::vector<int>(h.w_off, h.w_off + 8));
-    WOS_UP(slotv, h.slot_verts);
-#undef WOS_UP
+    struct Part {
+        const void *src;
+        size_t bytes;
+        size_t offset;
+    };
+    const std::vector<int> off(h.w_off, h.w_off + 8);
+    Part parts[] = {
+        {h.box64.data(), h.box64.size() * sizeof(double), 0},
+        {h.seg64.data(), h.seg64.size() * sizeof(double), 0},
+        {h.segid.data(), h.segid.size() * sizeof(int), 0},
+        {h.tri64.data(), h.tri64.size() * sizeof(double), 0},
+        {h.pair32.data(), h.pair32.size() * sizeof(float), 0},
+        {h.seg32.data(), h.seg32.size() * sizeof(float), 0},
+        {h.seg32inv.data(), h.seg32inv.size() * sizeof(float), 0},
+        {h.tri32.data(), h.tri32.size() * sizeof(float), 0},
+        {h.wbox.data(), h.wbox.size() * sizeof(float), 0},
+        {h.wprim.data(), h.wprim.size() * sizeof(float), 0},
+        {h.wide2bin.data(), h.wide2bin.size() * sizeof(int), 0},
+        {off.data(), off.size() * sizeof(int), 0},
+        {h.slot_verts.data(), h.slot_verts.size() * sizeof(int), 0},
+    };
+    size_t total = 0;
+    for (Part &p : parts) {
+        p.offset = total;
+        total += (std::max<size_t>(p.bytes, 16) + 255) / 256 * 256;
+    }
+    cudaError_t e = arena.reserve(total);
+    if (e != cudaSuccess) return e;
+    auto *base = static_cast<char *>(arena.ptr);
+    if ((e = cudaMemsetAsync(base, 0, total, stream)) != cudaSuccess) return e;
+    for (const Part &p : parts) {
+        if (p.bytes == 0) continue;
+        e = cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+    }
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    auto at = [&](int k) { return static_cast<const void *>(base + parts[k].offset); };
     view = SceneView{};
     view.dim = h.dim;
     view.n_prims = h.n_prims;
     view.depth = h.depth;
-    view.box64 = static_cast<const double *>(box64.ptr);
-    view.seg64 = static_cast<const double2 *>(seg64.ptr);
-    view.segid = static_cast<const int2 *>(segid.ptr);
-    view.tri64 = static_cast<const double2 *>(tri64.ptr);
-    view.pair32 = static_cast<const float4 *>(pair32.ptr);
-    view.seg32 = static_cast<const float4 *>(seg32.ptr);
-    view.seg32inv = static_cast<const float *>(seg32inv.ptr);
-    view.tri32 = static_cast<const float4 *>(tri32.ptr);
+    view.box64 = static_cast<const double *>(at(0));
+    view.seg64 = static_cast<const double2 *>(at(1));
+    view.segid = static_cast<const int2 *>(at(2));
+    view.tri64 = static_cast<const double2 *>(at(3));
+    view.pair32 = static_cast<const float4 *>(at(4));
+    view.seg32 = static_cast<const float4 *>(at(5));
+    view.seg32inv = static_cast<const float *>(at(6));
+    view.tri32 = static_cast<const float4 *>(at(7));
     wide = WideView{};
     wide.dim = h.dim;
     wide.H = h.wH;
     wide.n = h.n_prims;
     wide.npad = h.w_npad;
     wide.box_total = h.w_box_total;
-    wide.off = static_cast<const int *>(woff.ptr);
-    wide.box = static_cast<const float *>(wbox.ptr);
-    wide.prim = static_cast<const float *>(wprim.ptr);
-    wide.wide2bin = static_cast<const int *>(wide2bin.ptr);
+    wide.off = static_cast<const int *>(at(11));
+    wide.box = static_cast<const float *>(at(8));
+    wide.prim = static_cast<const float *>(at(9));
+    wide.wide2bin = static_cast<const int *>(at(10));
+    slot_verts = static_cast<const int *>(at(12));
     return build_lattice(h, stream);
 }
 
@@ -244,10 +257,9 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
 }
 
 void SceneDevice::release() {
-    for (DeviceBuffer *b : {&box64, &seg64, &segid, &tri64, &pair32, &seg32, &seg32inv, &tri32,
-                            &wbox, &wprim, &wide2bin, &woff, &slotv, &lattice}) {
-        b->release();
-    }
+    arena.release();
+    lattice.release();
+    slot_verts = nullptr;
 }
 
 int wos_context::upload_scene() {

@@ -22,10 +22,11 @@ struct DeviceBuffer {
 // Device copy of one HostScene (all tree and primitive arrays) and the
 // views the kernels take.
 struct SceneDevice {
-    DeviceBuffer box64, seg64, segid, tri64, pair32, seg32, seg32inv, tri32, wbox, wprim,
-        wide2bin, woff, slotv, lattice;
+    DeviceBuffer arena;    // every tree and primitive array, 256-byte aligned
+    DeviceBuffer lattice;  // the FAST_FP32 distance lattice
     SceneView view{};
     WideView wide{};
+    const int *slot_verts = nullptr;  // binary-tree slot -> the primitive's vertex ids
     // Uploads `h` on `stream` (synchronised) and fills view / wide.
     cudaError_t upload(const HostScene &h, cudaStream_t stream);
     // Builds the FAST_FP32 distance lattice into `lattice` and wide.gd.

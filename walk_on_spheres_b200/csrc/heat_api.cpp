@@ -152,7 +152,7 @@ int prepare_heat(wos_context *ctx, const wos_params *params, const wos_gaussian_
     const bool own = !(src->proposal_sigma > 0.0);
     for (int k = 0; k < 3; ++k) h.px0[k] = own ? src->x0[k] : src->proposal_x0[k];
     h.psigma = own ? src->sigma : src->proposal_sigma;
-    h.slot_verts = static_cast<const int *>(ctx->sdev.slotv.ptr);
+    h.slot_verts = ctx->sdev.slot_verts;
     if (vertex_values) {
         const size_t nv = static_cast<size_t>(ctx->scene.n_verts);
         WOS_CUDA(ctx, ctx->h_values.reserve(sizeof(double) * nv), "alloc vertex values");

@@ -400,7 +400,8 @@ cudaError_t batch_typed(int precision, int hc, const BatchItem *items, int n_ite
     if (precision == 32) {
         return with_height_class(hc, [&](auto h) {
             constexpr int HC = decltype(h)::value;
-            walk_batch_kernel<DIM, Eq, float, 3, HC><<<blocks, 256, 0, stream>>>(
+            constexpr int kMinBlocks = (HC == kHeightUpTo2 || HC == kHeight3) ? 4 : 3;
+            walk_batch_kernel<DIM, Eq, float, kMinBlocks, HC><<<blocks, 256, 0, stream>>>(
                 items, n_items, n_tasks, queue);
             return cudaGetLastError();
         });
@@ -417,8 +418,9 @@ cudaError_t batch_blocks_typed(int precision, int hc, int &blocks) {
     if (precision == 32) {
         e = with_height_class(hc, [&](auto h) {
             constexpr int HC = decltype(h)::value;
+            constexpr int kMinBlocks = (HC == kHeightUpTo2 || HC == kHeight3) ? 4 : 3;
             return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, walk_batch_kernel<DIM, Eq, float, 3, HC>, 256, 0);
+                &per_sm, walk_batch_kernel<DIM, Eq, float, kMinBlocks, HC>, 256, 0);
         });
     } else {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -607,13 +609,17 @@ __global__ void special32_kernel(const double *x, long long n, double *li0, doub
 }  // namespace
 
 namespace {
-// One lattice node per warp: the exact (keep = 1) FP32 cooperative query at
-// the node's FP32 position glo + (i, j, k) gh, the same position the walks'
-// lattice_sample rebuilds.  `margin` covers the FP32 rounding of the
-// primitive distances (a few ulps of the coordinates); sqrtf is correctly
-// rounded and the factor below takes it down.
+// One lattice node per warp: the FP32 cooperative query at the node's FP32
+// position glo + (i, j, k) gh, the same position the walks' lattice_sample
+// rebuilds.  The query prunes conservatively (keep = (1 - tau)^2, as the
+// walks do above the shell): it returns a squared distance at most
+// 1 / keep times the true one, and a node deep inside a round mesh, nearly
+// equidistant from every primitive, does not visit them all.  So the value
+// stored is sqrt(best) (1 - tau) minus `margin` (the FP32 rounding of the
+// primitive distances, a few ulps of the coordinates), rounded down.
 template <int DIM>
 __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin, float *out) {
+    constexpr float kShrink = 1.0f - 0x1p-10f;
     const int lane = threadIdx.x & 31;
     const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
@@ -626,9 +632,9 @@ __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin
         const float x = w.glo[0] + static_cast<float>(i) * w.gh;
         const float y = w.glo[1] + static_cast<float>(j) * w.gh;
         const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-        const WideResult q = wide_nearest<DIM>(w, x, y, z, 1.0f, 0.0f);
+        const WideResult q = wide_nearest<DIM>(w, x, y, z, kShrink * kShrink, 0.0f);
         if (lane == 0) {
-            const float d = (sqrtf(q.best) - margin) * (1.0f - 0x1p-20f);
+            const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
             out[t] = d > 0.0f ? d : 0.0f;
         }
     }

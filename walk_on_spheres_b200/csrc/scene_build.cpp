@@ -10,10 +10,6 @@
 
 namespace wosb {
 
-namespace {
-
-// Host threads of a build: WOS_HOST_THREADS when set to a positive count,
-// else the hardware's.
 unsigned host_threads() {
     static const unsigned t = [] {
         if (const char *e = std::getenv("WOS_HOST_THREADS")) {
@@ -24,6 +20,8 @@ unsigned host_threads() {
     }();
     return t;
 }
+
+namespace {
 
 // Subtree recursions split into host threads down to this depth (2^depth
 // threads at most); below it, or under kSerialItems items, they run inline.
@@ -404,6 +402,42 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
         float *blk = sc.wprim.data() + static_cast<size_t>(s / 32) * na * 32;
         for (int k = 0; k < na; ++k) blk[k * 32 + s % 32] = rec[k];
     }
+}
+
+std::string check_mesh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                       int leaf_size) {
+    if (dim != 2 && dim != 3) return "mesh dimension must be 2 or 3";
+    if (!verts || n_verts <= 0) return "mesh contains no vertices";
+    if (!prims || n_prims <= 0) {
+        return dim == 2 ? "mesh contains no line primitives" : "mesh contains no triangle primitives";
+    }
+    if (leaf_size == 0) leaf_size = 4;
+    if (leaf_size < 2 || leaf_size > 8) return "leaf_size must be 0 or in [2, 8]";
+    for (long long i = 0; i < static_cast<long long>(n_verts) * dim; ++i) {
+        if (!std::isfinite(verts[i])) return "vertex coordinates must be finite";
+    }
+    for (long long i = 0; i < static_cast<long long>(n_prims) * dim; ++i) {
+        if (prims[i] < 0 || prims[i] >= n_verts) return "primitive vertex index out of range";
+    }
+    auto V = [&](int v, int k) { return verts[static_cast<size_t>(dim) * v + k]; };
+    for (int p = 0; p < n_prims; ++p) {
+        if (dim == 2) {
+            const int a = prims[2 * p], b = prims[2 * p + 1];
+            const double dx = V(b, 0) - V(a, 0), dy = V(b, 1) - V(a, 1);
+            if (!(dx * dx + dy * dy > 0.0)) return "mesh contains a zero-length line segment";
+        } else {
+            const int a = prims[3 * p], b = prims[3 * p + 1], c = prims[3 * p + 2];
+            const double abx = V(b, 0) - V(a, 0), aby = V(b, 1) - V(a, 1), abz = V(b, 2) - V(a, 2);
+            const double acx = V(c, 0) - V(a, 0), acy = V(c, 1) - V(a, 1), acz = V(c, 2) - V(a, 2);
+            const double cx = aby * acz - abz * acy, cy = abz * acx - abx * acz,
+                         cz = abx * acy - aby * acx;
+            if (!(cx * cx + cy * cy + cz * cz > 0.0)) return "mesh contains a degenerate triangle";
+        }
+    }
+    int D = 0;
+    while (((static_cast<long long>(n_prims) + (1ll << D) - 1) >> D) > leaf_size) ++D;
+    if (D > 30) return "mesh too large for the BVH layout";
+    return std::string();
 }
 
 std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,

@@ -42,6 +42,15 @@ struct HostScene {
 // Validates the mesh like src/mesh.cpp:239-267 (no zero-length segment, no
 // degenerate triangle, indices in range) and builds the scene.  Returns an
 // empty string on success, otherwise the error message.
+// The checks of build_scene alone (same messages, same order), for callers
+// that validate a mesh now and build its trees later.
+std::string check_mesh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                       int leaf_size);
+
+// Host threads a build may use: WOS_HOST_THREADS when set to a positive
+// count, else the hardware's.
+unsigned host_threads();
+
 std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                         const int *boundary_ids, int leaf_size, HostScene &out);
 
