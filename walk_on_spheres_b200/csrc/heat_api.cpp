@@ -60,6 +60,7 @@ int wos_context::run_heat(const wos_params &p, const HeatDesc &h, const PointSet
     WOS_CUDA(this, cudaMemcpyAsync(&hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, stream),
              "read counters");
     WOS_CUDA(this, cudaStreamSynchronize(stream), "heat solve");
+    if (hc.error_flags) return fail(this, WOS_ERR_DEVICE, device_error(hc.error_flags));
     if (counters_out) {
         wos_counters &c = *counters_out;
         std::memset(&c, 0, sizeof(c));

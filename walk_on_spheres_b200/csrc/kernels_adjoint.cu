@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             for (int k = 0; k < 10; ++k) s_acc[k][threadIdx.x] = 0.0;
         }
         unsigned hits = 0;
+        bool bad = false;  // a closest-point query found no primitive
 
         int walk = w0 + lane;
         bool active = walk < w1;
@@ -297,31 +298,40 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                     np = np64;
                     bslot = slot64;
                 } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
-                    bslot = wv.wide2bin[slot];
-                    const double d64 = reproject64<DIM>(a.s, bslot, static_cast<double>(p.x),
-                                                        static_cast<double>(p.y),
-                                                        static_cast<double>(p.z), np, bid);
-                    if (d64 <= eps) {
+                    if (slot < 0) {  // a query found no primitive: flag it, stop
+                        bad = true;
                         stop = true;
                     } else {
-                        R = static_cast<T>(d64);
+                        bslot = wv.wide2bin[slot];
+                        const double d64 = reproject64<DIM>(
+                            a.s, bslot, static_cast<double>(p.x), static_cast<double>(p.y),
+                            static_cast<double>(p.z), np, bid);
+                        if (d64 <= eps) {
+                            stop = true;
+                        } else {
+                            R = static_cast<T>(d64);
+                        }
                     }
                 }
                 if (!stop && steps >= a.max_steps) {
                     ++hits;
                     stop = true;
                     if (kF32) {
-                        bslot = wv.wide2bin[slot];
-                        reproject64<DIM>(a.s, bslot, static_cast<double>(p.x),
-                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
-                                         bid);
+                        if (slot < 0) {
+                            bad = true;
+                        } else {
+                            bslot = wv.wide2bin[slot];
+                            reproject64<DIM>(a.s, bslot, static_cast<double>(p.x),
+                                             static_cast<double>(p.y), static_cast<double>(p.z),
+                                             np, bid);
+                        }
                     } else {
                         np = np64;
                         bslot = slot64;
                     }
                 }
                 if (stop) {
-                    value = sample + boundary_data<DIM>(a, bslot, np, cgrad);
+                    value = sample + (bslot >= 0 ? boundary_data<DIM>(a, bslot, np, cgrad) : 0.0);
                     done = true;
                 } else {
                     sample += heat_source<DIM, T>(a, p, R, rng, adj, j);
@@ -329,6 +339,18 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                     ++steps;
                     if constexpr (kF32) {
                         need_query = true;
+                        // the walk kernels' lattice step: away from the shell a
+                        // lattice lower bound is the radius (forward and replay
+                        // take the same branches, the lattice is fixed)
+                        if (wv.gd != nullptr && steps < a.max_steps) {
+                            const LatticeSample ls =
+                                lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
+                            const float gb = (ls.d - ls.r) * a.shrink;
+                            if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
+                                R = gb;
+                                need_query = false;
+                            }
+                        }
                     } else {
                         const Nearest<double> q = nearest64<DIM>(
                             a.s, static_cast<double>(p.x), static_cast<double>(p.y),
@@ -395,6 +417,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             }
         }
 
+        if (__ballot_sync(kFull, bad) && lane == 0) atomicOr(&a.ctr->error_flags, kErrBadState);
         double n_tot = static_cast<double>(n_acc);
         unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
 #pragma unroll
