@@ -65,8 +65,9 @@ UNIT = "walks/s"
 BYTES_PER_QUERY = 1863.4
 # DRAM bytes (read + write) of one walk-kernel launch of this workload, from a
 # one-pass ncu capture of the full launch (profiles/walk_fast_kernel_poisson2d_
-# circle1024.md): 6.21 MB and 6.25 MB for the two source modes.
-TRAFFIC_BYTES_PER_LAUNCH = 6.23e6
+# circle1024.md): 17.8 MB and 19.2 MB for the two source modes, most of it
+# the 16 MB distance lattice read once.
+TRAFFIC_BYTES_PER_LAUNCH = 18.5e6
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
 # 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in
 # the interior, 2048 FP32 walks each; one "gradient" is one full backward

@@ -11,8 +11,8 @@ from walk_on_spheres_b200 import meshes
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mname,G", [("circle1024", 1024), ("annulus", 1024), ("sphere", 96),
-                                     ("star", 1024)])
+@pytest.mark.parametrize("mname,G", [("circle1024", 2048), ("annulus", 2048), ("sphere", 160),
+                                     ("star", 2048)])
 def test_bounds_are_valid_and_tight(solver, mname, G):
     rng = np.random.default_rng(5)
     m = {"circle1024": meshes.circle(segments=1024), "annulus": meshes.annulus(),

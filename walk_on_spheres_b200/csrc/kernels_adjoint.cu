@@ -563,7 +563,10 @@ cudaError_t launch_heat_dim(const HeatArgs &a, int precision, const FastPlan &pl
         // forward and replay read the same tree, so they use one instantiation
         return with_height_class(height_class(a.w.H), [&](auto h) -> cudaError_t {
             constexpr int HC = decltype(h)::value;
-            auto k = heat_walk_kernel<DIM, float, 3, HC>;
+            // 4 blocks / SM (64 registers) for the height <= 3 traversals:
+            // the kernel waits on loads, so more resident warps pay
+            constexpr int kMinBlocks = (HC == kHeightUpTo2 || HC == kHeight3) ? 4 : 3;
+            auto k = heat_walk_kernel<DIM, float, kMinBlocks, HC>;
             // the static accumulators (20 KB) plus the staged scene can pass
             // the 48 KB default: opt in whenever anything is staged
             if (plan.smem_bytes > 0) {
