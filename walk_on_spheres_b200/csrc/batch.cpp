@@ -13,8 +13,10 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -115,31 +117,53 @@ struct wos_batch {
 };
 
 // Builds every pending mesh's trees on the host threads (one mesh per
-// thread, each build itself threaded for large meshes), then uploads them
-// and builds their lattices on the context's stream.
+// thread, largest first, each build itself threaded for large meshes) while
+// this thread uploads each finished mesh and builds its lattice on the
+// context's stream, so the device work overlaps the remaining builds.
 int wos_batch::prepare() {
     std::vector<BatchMesh *> todo;
     for (auto &m : meshes) {
         if (!m->built) todo.push_back(m.get());
     }
     if (todo.empty()) return WOS_OK;
+    std::stable_sort(todo.begin(), todo.end(), [](const BatchMesh *a, const BatchMesh *b) {
+        return a->prims.size() > b->prims.size();
+    });
     std::vector<std::string> errs(todo.size());
+    std::vector<char> done(todo.size(), 0);
+    std::mutex mu;
+    std::condition_variable cv;
     std::atomic<size_t> next{0};
     auto work = [&] {
         for (size_t i = next++; i < todo.size(); i = next++) {
             BatchMesh &m = *todo[i];
-            errs[i] = build_scene(m.dim, m.verts.data(), static_cast<int>(m.verts.size()) / m.dim,
-                                  m.prims.data(), static_cast<int>(m.prims.size()) / m.dim,
-                                  m.bids.empty() ? nullptr : m.bids.data(), m.leaf_size, m.scene);
+            std::string e =
+                build_scene(m.dim, m.verts.data(), static_cast<int>(m.verts.size()) / m.dim,
+                            m.prims.data(), static_cast<int>(m.prims.size()) / m.dim,
+                            m.bids.empty() ? nullptr : m.bids.data(), m.leaf_size, m.scene);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                errs[i] = std::move(e);
+                done[i] = 1;
+            }
+            cv.notify_all();
         }
     };
-    const size_t workers = std::min<size_t>(todo.size(), host_threads());
     std::vector<std::thread> pool;
-    for (size_t t = 1; t < workers; ++t) pool.emplace_back(work);
-    work();
-    for (std::thread &t : pool) t.join();
+    const size_t workers = std::min<size_t>(todo.size(), host_threads());
+    for (size_t t = 0; t < workers; ++t) pool.emplace_back(work);
+    struct Join {
+        std::vector<std::thread> &threads;
+        ~Join() {
+            for (std::thread &t : threads) t.join();
+        }
+    } join{pool};
     cudaSetDevice(ctx->device);
     for (size_t i = 0; i < todo.size(); ++i) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return done[i] != 0; });
+        }
         if (!errs[i].empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + errs[i]);
         BatchMesh &m = *todo[i];
         WOS_CUDA(ctx, m.dev.upload(m.scene, ctx->stream), "batch mesh upload");
