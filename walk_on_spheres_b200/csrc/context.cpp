@@ -177,7 +177,8 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
         e = cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return e;
     }
-    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    // no wait: a copy from pageable memory returns once its source is staged,
+    // and every later use of the scene is ordered after it on `stream`
     auto at = [&](int k) { return static_cast<const void *>(base + parts[k].offset); };
     view = SceneView{};
     view.dim = h.dim;
@@ -246,7 +247,6 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
     }
     auto *out = static_cast<float *>(lattice.ptr);
     if ((e = launch_lattice32(wide, margin, out, sms, stream)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     wide.gd = out;
     wide.gratio = 2.0f;  // bound >= 1/3 of the upper bound
     if (const char *env = std::getenv("WOS_LATTICE_RATIO")) {

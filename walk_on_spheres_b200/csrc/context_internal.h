@@ -27,7 +27,9 @@ struct SceneDevice {
     SceneView view{};
     WideView wide{};
     const int *slot_verts = nullptr;  // binary-tree slot -> the primitive's vertex ids
-    // Uploads `h` on `stream` (synchronised) and fills view / wide.
+    // Enqueues the upload of `h` and its lattice build on `stream` (no
+    // wait: later work on `stream` is ordered after them) and fills view /
+    // wide.
     cudaError_t upload(const HostScene &h, cudaStream_t stream);
     // Builds the FAST_FP32 distance lattice into `lattice` and wide.gd.
     cudaError_t build_lattice(const HostScene &h, cudaStream_t stream);

@@ -50,11 +50,12 @@ void both(int depth, int items, F &&left, G &&right) {
     }
 }
 
-// Runs f(i) for i in [0, n) on the host threads, in contiguous blocks.
+// Runs f(i) for i in [0, n) on the host threads, in contiguous blocks;
+// inline below `min_items` items (small loops of cheap items).
 template <class F>
-void parallel_for(long long n, F &&f) {
+void parallel_for(long long n, F &&f, long long min_items = 64) {
     const long long threads = host_threads();
-    if (n < 64 || threads == 1) {
+    if (n < min_items || n < 2 || threads == 1) {
         for (long long i = 0; i < n; ++i) f(i);
         return;
     }
@@ -299,7 +300,7 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
     for (int h = 1; h <= H; ++h) {
         cnt[h] = (cnt[h - 1] + 31) / 32;
         lv[h].assign(static_cast<size_t>(cnt[h]) * nc, 0.0);
-        for (long long i = 0; i < cnt[h]; ++i) {
+        parallel_for(cnt[h], [&](long long i) {
             const long long c0 = 32 * i, c1 = std::min(cnt[h - 1], 32 * i + 32);
             for (int k = 0; k < nc; ++k) {
                 double v = lv[h - 1][static_cast<size_t>(c0) * nc + k];
@@ -309,7 +310,7 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
                 }
                 lv[h][static_cast<size_t>(i) * nc + k] = v;
             }
-        }
+        });
     }
     // heights 1..H-1 are children of some node.  Children of one parent form
     // a group block of nbox x 32 floats (field f of child k at f*32 + k):
@@ -378,14 +379,15 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
             for (int k = 0; k < dim; ++k) blk[(nc + k) * 32 + lane] = nf[k];
             blk[(nc + dim) * 32 + lane] = cf;
             blk[(nc + dim + 1) * 32 + lane] = round_up(t32 + 4.0 * widen);
-        });
+        }, 2);  // the top heights have a few large nodes: thread them too
     }
     // primitives in wide-slot order, one block of na x 32 floats per cluster
     // (field f of slot 32c + k at c*na*32 + f*32 + k); padding primitives are
     // far away
     const int na = dim == 2 ? 5 : 16;
     sc.wprim.assign(static_cast<size_t>(sc.w_npad) * na, 0.0f);
-    for (int s = 0; s < sc.w_npad; ++s) {
+    parallel_for(sc.w_npad, [&](long long sl) {
+        const int s = static_cast<int>(sl);
         float rec[16];
         if (s >= n) {
             for (float &x : rec) x = 0.0f;
@@ -401,7 +403,7 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
         }
         float *blk = sc.wprim.data() + static_cast<size_t>(s / 32) * na * 32;
         for (int k = 0; k < na; ++k) blk[k * 32 + s % 32] = rec[k];
-    }
+    });
 }
 
 std::string check_mesh(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
@@ -531,7 +533,8 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
     const int rec = dim == 2 ? 8 : 12;
     const long long n_pairs = 1ll << D;  // parents 1 .. 2^D - 1 (record 0 unused)
     sc.pair32.assign(static_cast<size_t>(std::max<long long>(n_pairs, 1)) * rec, 0.0f);
-    for (long long i = 1; i < n_pairs; ++i) {
+    parallel_for(n_pairs, [&](long long i) {
+        if (i == 0) return;  // record 0 unused
         float *r = sc.pair32.data() + static_cast<size_t>(rec) * i;
         for (int side = 0; side < 2; ++side) {
             const double *b = sc.box64.data() + static_cast<size_t>(2 * dim) * (2 * i + side);
@@ -556,7 +559,7 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
                 o[5] = hi[2];
             }
         }
-    }
+    });
 
     // leaf-slot primitive records
     if (dim == 2) {
@@ -564,7 +567,8 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
         sc.segid.resize(static_cast<size_t>(n_prims) * 2);
         sc.seg32.resize(static_cast<size_t>(n_prims) * 4);
         sc.seg32inv.resize(static_cast<size_t>(n_prims));
-        for (int s = 0; s < n_prims; ++s) {
+        parallel_for(n_prims, [&](long long sl) {
+            const int s = static_cast<int>(sl);
             const int p = sc.order[s];
             const int a = prims[2 * p], b = prims[2 * p + 1];
             const double g[4] = {V(a, 0), V(a, 1), V(b, 0), V(b, 1)};
@@ -580,11 +584,12 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
                 1.0 / (static_cast<double>(vx) * vx + static_cast<double>(vy) * vy));
             sc.segid[2 * s] = sc.boundary_ids[p];
             sc.segid[2 * s + 1] = p;
-        }
+        });
     } else {
         sc.tri64.resize(static_cast<size_t>(n_prims) * 14);
         sc.tri32.resize(static_cast<size_t>(n_prims) * 16);
-        for (int s = 0; s < n_prims; ++s) {
+        parallel_for(n_prims, [&](long long sl) {
+            const int s = static_cast<int>(sl);
             const int p = sc.order[s];
             const int a = prims[3 * p], b = prims[3 * p + 1], c = prims[3 * p + 2];
             // Eberly cache, src/bvh.cpp:204-217
@@ -621,7 +626,7 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
             o[13] = static_cast<float>(1.0 / fdet);
             o[14] = static_cast<float>(1.0 / fa);
             o[15] = static_cast<float>(1.0 / fc);
-        }
+        });
     }
     sc.slot_verts.resize(static_cast<size_t>(n_prims) * dim);
     for (int s = 0; s < n_prims; ++s) {
