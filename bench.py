@@ -169,18 +169,27 @@ def workload_mesh():
 
 
 def scene_upload_bytes(mesh) -> int:
-    """Bytes wos_set_mesh copies host->device for a 2D mesh (device/scene.cuh layout)."""
+    """Bytes wos_set_mesh copies host->device for a 2D mesh: binary-tree boxes
+    (2^(D+1) x 4 doubles), FP64 segments (4 doubles) and {boundary id,
+    primitive} per slot, the 32-wide tree's child blocks, its primitive
+    blocks (5 floats per slot), wide-to-binary slot map, height offsets and
+    vertex ids per slot.  The distance lattice is built on the device."""
     from walk_on_spheres_b200 import _lib
     import ctypes as C
-    d = C.c_int()
+    L = _lib.lib()
+    d, H, E = C.c_int(), C.c_int(), C.c_int()
     verts = np.ascontiguousarray(mesh.verts)
     prims = np.ascontiguousarray(mesh.prims, dtype=np.int32)
-    _lib.lib().wos_build_bvh.restype = C.c_int
-    _lib.lib().wos_build_bvh(2, verts.ctypes.data_as(C.c_void_p), verts.shape[0],
-                             prims.ctypes.data_as(C.c_void_p), prims.shape[0], 0, C.byref(d),
-                             None, None)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    L.wos_build_bvh.restype = C.c_int
+    L.wos_build_bvh(2, vp(verts), verts.shape[0], vp(prims), prims.shape[0], 0, C.byref(d),
+                    None, None)
+    L.wos_build_wide_bvh(2, vp(verts), verts.shape[0], vp(prims), prims.shape[0], C.byref(H),
+                         C.byref(E), None, None, None)
     n, D = mesh.n_prims, d.value
-    return (2 ** (D + 1)) * 32 + n * 32 + n * 8 + (2 ** D) * 32 + n * 16
+    npad = (n + 31) // 32 * 32
+    return ((2 ** (D + 1)) * 32 + n * 32 + n * 8 + E.value * 4 + npad * 20 + npad * 4 + 32
+            + n * 8)
 
 
 def hbm_peak():

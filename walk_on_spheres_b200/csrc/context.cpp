@@ -153,10 +153,6 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
         {h.seg64.data(), h.seg64.size() * sizeof(double), 0},
         {h.segid.data(), h.segid.size() * sizeof(int), 0},
         {h.tri64.data(), h.tri64.size() * sizeof(double), 0},
-        {h.pair32.data(), h.pair32.size() * sizeof(float), 0},
-        {h.seg32.data(), h.seg32.size() * sizeof(float), 0},
-        {h.seg32inv.data(), h.seg32inv.size() * sizeof(float), 0},
-        {h.tri32.data(), h.tri32.size() * sizeof(float), 0},
         {h.wbox.data(), h.wbox.size() * sizeof(float), 0},
         {h.wprim.data(), h.wprim.size() * sizeof(float), 0},
         {h.wide2bin.data(), h.wide2bin.size() * sizeof(int), 0},
@@ -188,21 +184,17 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
     view.seg64 = static_cast<const double2 *>(at(1));
     view.segid = static_cast<const int2 *>(at(2));
     view.tri64 = static_cast<const double2 *>(at(3));
-    view.pair32 = static_cast<const float4 *>(at(4));
-    view.seg32 = static_cast<const float4 *>(at(5));
-    view.seg32inv = static_cast<const float *>(at(6));
-    view.tri32 = static_cast<const float4 *>(at(7));
     wide = WideView{};
     wide.dim = h.dim;
     wide.H = h.wH;
     wide.n = h.n_prims;
     wide.npad = h.w_npad;
     wide.box_total = h.w_box_total;
-    wide.off = static_cast<const int *>(at(11));
-    wide.box = static_cast<const float *>(at(8));
-    wide.prim = static_cast<const float *>(at(9));
-    wide.wide2bin = static_cast<const int *>(at(10));
-    slot_verts = static_cast<const int *>(at(12));
+    wide.off = static_cast<const int *>(at(7));
+    wide.box = static_cast<const float *>(at(4));
+    wide.prim = static_cast<const float *>(at(5));
+    wide.wide2bin = static_cast<const int *>(at(6));
+    slot_verts = static_cast<const int *>(at(8));
     return build_lattice(h, stream);
 }
 

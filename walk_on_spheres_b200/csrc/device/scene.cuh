@@ -24,13 +24,8 @@
 //   segid  2D per slot {boundary_id, primitive id}
 //   tri64  3D FP64 Eberly records per slot, 7 double2: v0, e1, e2, a, b, c,
 //          det, denom (values of src/bvh.cpp:204-217)
-//   pair32 FP32 child-box pairs by parent id: 2D 2 float4 {lo.x,lo.y,hi.x,hi.y}
-//          (left, right); 3D 3 float4 packing left lo/hi then right lo/hi.
-//          Boxes are the FP64 boxes rounded outward and widened by 2^-20 of
-//          the mesh scale, so they bound the FP32 primitives.
-//   seg32  2D FP32 segments per slot {x0, y0, vx, vy}, seg32inv 1/|v|^2
-//   tri32  3D FP32 Eberly records per slot, 4 float4:
-//          {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}
+// The FP32 fast path queries the 32-wide tree of wide.cuh instead, whose
+// primitive blocks hold FP32 records (eberly32 below reads the 3D one).
 #pragma once
 #include <cstdint>
 
@@ -46,10 +41,6 @@ struct SceneView {
     const double2 *seg64;
     const int2 *segid;
     const double2 *tri64;
-    const float4 *pair32;  // 2^D pair records (id 0 unused), 2 or 3 float4 each
-    const float4 *seg32;
-    const float *seg32inv;  // 2D: 1 / |v|^2 per slot
-    const float4 *tri32;
 };
 
 __host__ __device__ __forceinline__ int leaf_first(int j, int n, int depth) {
@@ -306,69 +297,7 @@ __device__ __forceinline__ Nearest<double> nearest64(const SceneView &s, double 
     return q;
 }
 
-// ---- FP32 policies ----------------------------------------------------------
-
-__device__ __forceinline__ float box_dist32_2(float4 b, float px, float py) {
-    const float dx = fmaxf(0.0f, fmaxf(b.x - px, px - b.z));
-    const float dy = fmaxf(0.0f, fmaxf(b.y - py, py - b.w));
-    return dx * dx + dy * dy;
-}
-
-__device__ __forceinline__ float box_dist32_3(float lx, float ly, float lz, float hx, float hy,
-                                              float hz, float px, float py, float pz) {
-    const float dx = fmaxf(0.0f, fmaxf(lx - px, px - hx));
-    const float dy = fmaxf(0.0f, fmaxf(ly - py, py - hy));
-    const float dz = fmaxf(0.0f, fmaxf(lz - pz, pz - hz));
-    return dx * dx + dy * dy + dz * dz;
-}
-
-// Result of an FP32 query: squared distance, pruning bound and winning slot.
-// Above `exact2` the bound is best * keep with keep = (1 - tau)^2: nodes that
-// could improve the distance by less than a relative tau are skipped, so the
-// true distance d satisfies (1 - tau) sqrt(best) <= d <= sqrt(best) and
-// (1 - tau) sqrt(best) is a radius whose ball lies inside the domain.  Below
-// `exact2` (inside the epsilon shell) pruning is exact.
-struct Nearest32 {
-    float best;
-    float limit;
-    float keep;
-    float exact2;
-    int slot;
-    __device__ __forceinline__ void offer(float d2, int k) {
-        if (d2 < best) {
-            best = d2;
-            slot = k;
-            limit = d2 > exact2 ? d2 * keep : d2;
-        }
-    }
-};
-
-// 2D FP32 segments: {x0, y0, vx, vy} plus 1/|v|^2 per slot.
-struct Seg32Policy {
-    const float4 *pairs;
-    const float4 *segs;
-    const float *inv;
-    int n, depth;
-    float px, py;
-    __device__ __forceinline__ float node_dist(unsigned id) const {
-        return box_dist32_2(pairs[2 * (id >> 1) + (id & 1u)], px, py);
-    }
-    __device__ __forceinline__ void child_dists(unsigned id, float &dl, float &dr) const {
-        dl = box_dist32_2(pairs[2 * id], px, py);
-        dr = box_dist32_2(pairs[2 * id + 1], px, py);
-    }
-    __device__ __forceinline__ void test_leaf(int j, Nearest32 &q) const {
-        const int b = leaf_first(j, n, depth);
-        const int e = leaf_first(j + 1, n, depth);
-        for (int k = b; k < e; ++k) {
-            const float4 g = segs[k];
-            const float wx = px - g.x, wy = py - g.y;
-            const float t = fminf(fmaxf((wx * g.z + wy * g.w) * inv[k], 0.0f), 1.0f);
-            const float dx = wx - t * g.z, dy = wy - t * g.w;
-            q.offer(dx * dx + dy * dy, k);
-        }
-    }
-};
+// ---- FP32 primitive test ----------------------------------------------------
 
 // Eberly's regions in FP32 with precomputed reciprocals; returns the squared
 // distance only.  Record: {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}.
@@ -428,56 +357,6 @@ __device__ __forceinline__ float eberly32(float px, float py, float pz, const fl
     const float dy = bpy + s * B.y + t * C.y;
     const float dz = bpz + s * B.z + t * C.z;
     return dx * dx + dy * dy + dz * dz;
-}
-
-struct Tri32Policy {
-    const float4 *pairs;
-    const float4 *tris;
-    int n, depth;
-    float px, py, pz;
-    __device__ __forceinline__ float node_dist(unsigned id) const {
-        const float4 *r = pairs + 3 * (id >> 1);
-        if ((id & 1u) == 0) {
-            const float4 a = r[0], b = r[1];
-            return box_dist32_3(a.x, a.y, a.z, a.w, b.x, b.y, px, py, pz);
-        }
-        const float4 b = r[1], c = r[2];
-        return box_dist32_3(b.z, b.w, c.x, c.y, c.z, c.w, px, py, pz);
-    }
-    __device__ __forceinline__ void child_dists(unsigned id, float &dl, float &dr) const {
-        const float4 *r = pairs + 3 * id;
-        const float4 a = r[0], b = r[1], c = r[2];
-        dl = box_dist32_3(a.x, a.y, a.z, a.w, b.x, b.y, px, py, pz);
-        dr = box_dist32_3(b.z, b.w, c.x, c.y, c.z, c.w, px, py, pz);
-    }
-    __device__ __forceinline__ void test_leaf(int j, Nearest32 &q) const {
-        const int b = leaf_first(j, n, depth);
-        const int e = leaf_first(j + 1, n, depth);
-        for (int k = b; k < e; ++k) q.offer(eberly32(px, py, pz, tris + 4 * k), k);
-    }
-};
-
-// FP32 closest-point query through the given pair / primitive arrays (global
-// or shared memory), conservative to a relative tolerance tau above the exact
-// radius sqrt(exact2) (see Nearest32).
-template <int DIM>
-__device__ __forceinline__ Nearest32 nearest32(const float4 *pairs, const float4 *prims,
-                                               const float *inv, int n, int depth, float px,
-                                               float py, float pz, float keep, float exact2) {
-    Nearest32 q;
-    q.best = INFINITY;
-    q.limit = INFINITY;
-    q.keep = keep;
-    q.exact2 = exact2;
-    q.slot = -1;
-    if (DIM == 2) {
-        Seg32Policy P{pairs, prims, inv, n, depth, px, py};
-        traverse_nearest<float>(P, depth, q);
-    } else {
-        Tri32Policy P{pairs, prims, n, depth, px, py, pz};
-        traverse_nearest<float>(P, depth, q);
-    }
-    return q;
 }
 
 // --------------------------------------------------------------------------

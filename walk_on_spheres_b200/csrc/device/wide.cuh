@@ -22,8 +22,13 @@
 // keeps the children whose key is above the one just left, which are exactly
 // the pending ones because children are taken in increasing key order.
 //
-// Pruning is conservative to a relative tau above the epsilon shell (see
-// Nearest32 in scene.cuh): bound = best * keep while best > exact2.
+// Pruning is conservative to a relative tau above the epsilon shell: while
+// best > exact2 a node is skipped when its bound exceeds best * keep, with
+// keep = (1 - tau)^2, so nodes that could improve the distance by less than a
+// relative tau are skipped and the true distance d satisfies
+// (1 - tau) sqrt(best) <= d <= sqrt(best); (1 - tau) sqrt(best) is then a
+// radius whose ball lies inside the domain.  Below exact2 (inside the
+// epsilon shell) pruning is exact.
 #pragma once
 #include <cstdint>
 #include <type_traits>

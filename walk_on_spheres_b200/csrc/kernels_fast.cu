@@ -731,7 +731,7 @@ FastArgs make_fast_args(const SceneView &s, const WideView &w, const PointSet &p
     a.stage_box = 0;
     a.stage_prim = 0;
     // FP32 queries are conservative to a relative tau = 2^-10 outside the
-    // epsilon shell and exact inside it (see Nearest32)
+    // epsilon shell and exact inside it (see wide_nearest)
     const double tau = 1.0 / 1024.0;
     const double shell = epsilon + shell_delta;
     a.keep = static_cast<float>((1.0 - tau) * (1.0 - tau));

@@ -528,39 +528,6 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
     sc.order.resize(n_prims);
     for (int s = 0; s < n_prims; ++s) sc.order[s] = B.items[s].prim;
 
-    // FP32 child-pair boxes: outward-rounded FP64 boxes widened by 2^-20 * scale
-    const double widen = std::ldexp(sc.scale, -20);
-    const int rec = dim == 2 ? 8 : 12;
-    const long long n_pairs = 1ll << D;  // parents 1 .. 2^D - 1 (record 0 unused)
-    sc.pair32.assign(static_cast<size_t>(std::max<long long>(n_pairs, 1)) * rec, 0.0f);
-    parallel_for(n_pairs, [&](long long i) {
-        if (i == 0) return;  // record 0 unused
-        float *r = sc.pair32.data() + static_cast<size_t>(rec) * i;
-        for (int side = 0; side < 2; ++side) {
-            const double *b = sc.box64.data() + static_cast<size_t>(2 * dim) * (2 * i + side);
-            float lo[3], hi[3];
-            for (int k = 0; k < dim; ++k) {
-                lo[k] = round_down(b[k] - widen);
-                hi[k] = round_up(b[dim + k] + widen);
-            }
-            if (dim == 2) {
-                float *o = r + 4 * side;
-                o[0] = lo[0];
-                o[1] = lo[1];
-                o[2] = hi[0];
-                o[3] = hi[1];
-            } else {
-                float *o = r + 6 * side;
-                o[0] = lo[0];
-                o[1] = lo[1];
-                o[2] = lo[2];
-                o[3] = hi[0];
-                o[4] = hi[1];
-                o[5] = hi[2];
-            }
-        }
-    });
-
     // leaf-slot primitive records
     if (dim == 2) {
         sc.seg64.resize(static_cast<size_t>(n_prims) * 4);

@@ -18,7 +18,8 @@ struct HostScene {
     std::vector<double> seg64;   // 2D: 4 per slot
     std::vector<int> segid;      // 2D: {boundary_id, prim} per slot
     std::vector<double> tri64;   // 3D: 14 per slot
-    std::vector<float> pair32;   // 2^D records of 8 (2D) or 12 (3D) floats
+    // FP32 records per binary slot (host only: the wide primitive blocks
+    // are filled from them)
     std::vector<float> seg32;    // 2D: {x0, y0, vx, vy} per slot
     std::vector<float> seg32inv; // 2D: 1/|v|^2 per slot
     std::vector<float> tri32;    // 3D: {v0, a} {e1, b} {e2, c} {det, 1/det, 1/a, 1/c}
