@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <thread>
+#include <utility>
 
 namespace wosb {
 
@@ -599,7 +600,7 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
     for (int s = 0; s < n_prims; ++s) {
         for (int k = 0; k < dim; ++k) sc.slot_verts[dim * s + k] = prims[dim * sc.order[s] + k];
     }
-    build_wide(sc, B.items, dim);
+    build_wide(sc, std::move(B.items), dim);  // the binary build is done with them
     return std::string();
 }
 
