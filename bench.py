@@ -448,6 +448,9 @@ def gpu_arm(args, rank, world, local):
         "variance_ratio_fp64_over_fast": var_ratio,
         "plain_fp64_walks_per_s": plain_rate,
         "speedup_vs_plain_fp64_matched_se": value / plain_rate if plain_rate else None,
+        # walk steps: each is one closest-point query of the reference's
+        # algorithm; FAST_FP32 answers most of them with a distance-lattice
+        # bound instead of a BVH query
         "closest_point_queries_per_s": (steps_total / job_s) * (world if dist else 1),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
