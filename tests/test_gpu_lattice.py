@@ -11,7 +11,7 @@ from walk_on_spheres_b200 import meshes
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mname,G", [("circle1024", 2048), ("annulus", 2048), ("sphere", 160),
+@pytest.mark.parametrize("mname,G", [("circle1024", 2048), ("annulus", 2048), ("sphere", 256),
                                      ("star", 2048)])
 def test_bounds_are_valid_and_tight(solver, mname, G):
     rng = np.random.default_rng(5)

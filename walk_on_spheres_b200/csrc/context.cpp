@@ -200,7 +200,7 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
 
 // The distance lattice of the FAST_FP32 walks (device/wide.cuh): nodes
 // spaced h = (largest bbox extent) / (G - 1) over the bounding box, G = 2048
-// in 2D and 160 in 3D (16 MB each for a square / cubic box), distances
+// in 2D and 256 in 3D (16 MB and 64 MB for a square / cubic box), distances
 // from the exact FP32 cooperative query at the nodes' FP32 positions.
 // Meshes of at most lane_prims primitives query exactly at every step and get
 // none; WOS_BOUND_GRID=0 turns it off.
@@ -210,7 +210,7 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
     if (const char *env = std::getenv("WOS_BOUND_GRID")) {
         if (std::string(env) == "0") return cudaSuccess;
     }
-    const int G = h.dim == 2 ? 2048 : 160;
+    const int G = h.dim == 2 ? 2048 : 256;
     double ext = 0.0, mag = 0.0;
     for (int k = 0; k < h.dim; ++k) {
         ext = std::max(ext, h.bbox[2 * k + 1] - h.bbox[2 * k]);

@@ -617,7 +617,7 @@ namespace {
 // equidistant from every primitive, does not visit them all.  So the value
 // stored is sqrt(best) (1 - tau) minus `margin` (the FP32 rounding of the
 // primitive distances, a few ulps of the coordinates), rounded down.
-template <int DIM>
+template <int DIM, int HC>
 __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin, float *out) {
     constexpr float kShrink = 1.0f - 0x1p-10f;
     const int lane = threadIdx.x & 31;
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin
         const float x = w.glo[0] + static_cast<float>(i) * w.gh;
         const float y = w.glo[1] + static_cast<float>(j) * w.gh;
         const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-        const WideResult q = wide_nearest<DIM>(w, x, y, z, kShrink * kShrink, 0.0f);
+        const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, kShrink * kShrink, 0.0f);
         if (lane == 0) {
             const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
             out[t] = d > 0.0f ? d : 0.0f;
@@ -660,12 +660,18 @@ cudaError_t launch_lattice32(const WideView &w, float margin, float *out, int sm
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
     if (n <= 0) return cudaSuccess;
     const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
-    if (w.dim == 2) {
-        lattice32_kernel<2><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
-    } else {
-        lattice32_kernel<3><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
-    }
-    return cudaGetLastError();
+    // compiled per traversal class, like the walk kernels
+    return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
+        constexpr int HC = decltype(h)::value;
+        if (w.dim == 2) {
+            lattice32_kernel<2, HC>
+                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+        } else {
+            lattice32_kernel<3, HC>
+                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+        }
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
