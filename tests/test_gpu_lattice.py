@@ -12,11 +12,13 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("mname,G", [("circle1024", 2048), ("annulus", 2048), ("sphere", 256),
-                                     ("star", 2048)])
+                                     ("star", 2048), ("slab", 256)])
 def test_bounds_are_valid_and_tight(solver, mname, G):
     rng = np.random.default_rng(5)
     m = {"circle1024": meshes.circle(segments=1024), "annulus": meshes.annulus(),
-         "sphere": meshes.uv_sphere(), "star": meshes.star_polygon(rng, 3000)}[mname]
+         "sphere": meshes.uv_sphere(), "star": meshes.star_polygon(rng, 3000),
+         # thin and anisotropic: 0.10 x 0.05 x 0.01 m, cells of 0.4 mm
+         "slab": meshes.slab_box(target_triangles=20000)}[mname]
     solver.set_mesh(m)
     lo, hi = np.asarray(solver.bbox[0::2][:m.dim]), np.asarray(solver.bbox[1::2][:m.dim])
     pts = lo + (hi - lo) * rng.random((20000, m.dim))
