@@ -277,10 +277,14 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
     FastPlan plan{};
     if (p.method != WOS_METHOD_PLAIN_FP64) {
         plan = plan_fast(dev.view, dev.wide, n, p.walks, precision, ctx->sms, ctx->smem_optin);
-        // a step is small: cut walks into chunks that give ~8 waves of tasks
+        // a step is small: about two waves of tasks, and at least 256 walks
+        // (8 per lane) per task so that a lane whose walk ends takes the
+        // next one.  At the level-2 defaults 32 walks per task (one per
+        // lane) left a warp waiting for its longest walk: 276 ms for the
+        // run, against 184 ms at 256.
         const long long resident = static_cast<long long>(ctx->sms) * 24;
-        long long chunk = static_cast<long long>(p.walks) * n / (8 * resident);
-        chunk = std::max<long long>(32, std::min<long long>(1024, chunk));
+        long long chunk = static_cast<long long>(p.walks) * n / (2 * resident);
+        chunk = std::max<long long>(256, std::min<long long>(1024, chunk));
         if (ctx->chunk_override > 0) chunk = ctx->chunk_override;
         plan.chunk = static_cast<int>(std::min<long long>(chunk, p.walks));
         plan.chunks = (p.walks + plan.chunk - 1) / plan.chunk;
