@@ -16,6 +16,8 @@ Tolerances:
   per-step standard error does not include, so they are compared through
   the field's total (2% at 2000 walks).
 * graph replay and stream launch: bit-for-bit equal.
+* FAST_FP32 / FAST_FP64 at the level-2 defaults pass the reference's own
+  level-2 validation (oracle/fd_transient.py).
 """
 from __future__ import annotations
 
@@ -116,3 +118,19 @@ def test_rejects_the_reference_invalid_configurations(solver):
         solve_transient(solver, heat_on_time=10.0, total_time=10.0)
     with pytest.raises(WosError, match="integer multiple"):
         solve_transient(solver, dt=0.3, total_time=1.0, heat_on_time=0.5)
+
+
+@pytest.mark.parametrize("method", ["fast", "fast64"])
+def test_fast_passes_the_reference_level2_validation(solver, method):
+    # apps/welding/tools/validate_level2.py restated in oracle/fd_transient.py:
+    # at the reference's level-2 defaults (49 x 33, 100 steps, 500 walks)
+    # every step's field is within 5% RMS and 10% at the centre of the
+    # implicit finite-difference solution, relative to its peak
+    from oracle.fd_transient import level2_gates
+    from walk_on_spheres_b200.transient import defaults, solve_transient
+    r = solve_transient(solver, method=method)
+    params = defaults()
+    g = level2_gates(r.fields, r.standard_error, params, r.max_steps_hits)
+    assert g["passed"], g["failures"][:5]
+    worst = max(row["normalized_rmse"] for row in g["rows"])
+    assert worst < 0.05, worst

@@ -64,3 +64,42 @@ def test_level_presets_are_valid():
     assert L.wos_transient_steps(C.byref(make_params(**LEVEL3))) == 150
     f = level0_initial()
     assert f.shape == (17, 17) and abs(f[8, 8] - 1.0) < 1e-15 and f[0].max() == 0.0
+
+
+def test_fd_reference_modes_match_a_dense_solve():
+    # the sine-mode implicit step equals a dense solve of
+    # (I - c Lap_h) u = rhs with u = 0 on the grid edges
+    from oracle.fd_transient import SineModes
+    nx, ny, dx, dy, c = 9, 7, 0.1, 0.07, 0.03
+    mx, my = nx - 2, ny - 2
+    A = np.zeros((mx * my, mx * my))
+    for i in range(mx):
+        for j in range(my):
+            r = i * my + j
+            A[r, r] = 1.0 + c * (2.0 / dx**2 + 2.0 / dy**2)
+            for di, dj, h in ((1, 0, dx), (-1, 0, dx), (0, 1, dy), (0, -1, dy)):
+                ii, jj = i + di, j + dj
+                if 0 <= ii < mx and 0 <= jj < my:
+                    A[r, ii * my + jj] -= c / h**2
+    rhs = np.random.default_rng(3).random((mx, my))
+    want = np.linalg.solve(A, rhs.ravel()).reshape(mx, my)
+    m = SineModes(nx, ny, dx, dy, c)
+    got = m.inverse(m.forward(rhs) / m.denominator)
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-13)
+
+
+def test_fd_reference_heats_then_cools():
+    # level-2 defaults: the FD field rises while the source is on and decays
+    # after; the energy injected is the absorbed power times heat_on_time
+    from oracle.fd_transient import fd_fields, heating_fraction
+    p = defaults()
+    f = fd_fields(p)
+    steps = f.shape[0] - 1
+    on = int(round(p["heat_on_time"] / p["dt"]))
+    c = (p["nx"] // 2, p["ny"] // 2)
+    assert f[on][c] > f[on // 2][c] > 0.0 and f[steps][c] < f[on][c]
+    assert np.all(f[:, 0, :] == 0.0) and np.all(f[:, :, -1] == 0.0)
+    absorbed = p["electrical_power"] * p["efficiency"]
+    energy = sum(absorbed * heating_fraction((s - 1) * p["dt"], s * p["dt"], p["heat_on_time"])
+                 * p["dt"] for s in range(1, steps + 1))
+    assert abs(energy - absorbed * p["heat_on_time"]) < 1e-9
