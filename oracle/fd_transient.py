@@ -1,6 +1,9 @@
-"""Finite-difference reference of the transient plate problem (welding level 2)
-and the reference's level-2 validation gates.  TEST INFRASTRUCTURE ONLY: the
-checker of the transient solver, never part of the product path.
+"""Finite-difference references of the transient plate problems (welding
+levels 2 and 3) and the reference's validation gates.  TEST INFRASTRUCTURE
+ONLY: the checker of the transient solver, never part of the product path.
+
+Level 3 (moving source): fd_fields_moving / level3_gates restate
+apps/welding/tools/validate_level3.py:133-420 (below).
 
 Restates apps/welding/tools/validate_level2.py:108-330 (default options: the
 WoS grid itself, one implicit step per WoS step):
@@ -120,3 +123,117 @@ def level2_gates(fields: np.ndarray, standard_error: np.ndarray, params: dict,
         if ncentre > center_limit:
             failures.append(f"step {s}: normalized centre error {ncentre:.3%}")
     return {"rows": rows, "failures": failures, "passed": not failures}
+
+
+# ---------------------------------------------------------------- level 3
+
+# the program's fixed probes (level3_moving_heat.cpp:85-93): name, x, y
+LEVEL3_PROBES = (("centreline_m20", -0.020, 0.000), ("centreline_m10", -0.010, 0.000),
+                 ("centreline_0", 0.000, 0.000), ("centreline_p10", 0.010, 0.000),
+                 ("centreline_p20", 0.020, 0.000), ("transverse_p5", 0.000, 0.005),
+                 ("transverse_p10", 0.000, 0.010))
+
+
+def fd_fields_moving(params: dict, refinement: int = 4, substeps: int = 16) -> np.ndarray:
+    """FD temperature rise of the moving-source problem at the WoS nodes of
+    every step, shape (steps + 1, nx, ny) (validate_level3.py:133-240): a
+    grid refined `refinement` times, `substeps` implicit steps per WoS step,
+    the source sampled at each substep's midpoint while it is on."""
+    nx, ny, dt = params["nx"], params["ny"], params["dt"]
+    steps = int(round(params["total_time"] / dt))
+    x0, y0 = params["plate_x0"], params["plate_y0"]
+    lx, ly = params["length_x"], params["length_y"]
+    rnx, rny = (nx - 1) * refinement + 1, (ny - 1) * refinement + 1
+    rx, ry = np.linspace(x0, x0 + lx, rnx), np.linspace(y0, y0 + ly, rny)
+    heat_capacity = params["density"] * params["specific_heat"]
+    kappa = params["conductivity"] / heat_capacity
+    rdt = dt / substeps
+    modes = SineModes(rnx, rny, rx[1] - rx[0], ry[1] - ry[0], kappa * rdt)
+    sx, sy = params["sigma_x"], params["sigma_y"]
+    wy = params["weld_y"]
+    absorbed = params["electrical_power"] * params["efficiency"]
+    iy = gaussian_integral(y0, y0 + ly, wy, sy)
+    proj_y = modes.sy.T @ np.exp(-0.5 * ((ry[1:-1] - wy) / sy) ** 2)
+    c = np.zeros((rnx - 2, rny - 2))
+    out = np.zeros((steps + 1, nx, ny))
+    for s in range(1, steps + 1):
+        for k in range(substeps):
+            tm = (s - 1) * dt + (k + 0.5) * rdt
+            if tm < params["heat_on_time"]:
+                cx = params["source_start_x"] + params["weld_speed"] * tm
+                ix = gaussian_integral(x0, x0 + lx, cx, sx)
+                proj_x = modes.sx.T @ np.exp(-0.5 * ((rx[1:-1] - cx) / sx) ** 2)
+                amp = absorbed / (params["thickness"] * ix * iy * heat_capacity)
+                c = (c + rdt * modes.scale * amp * np.outer(proj_x, proj_y)) / modes.denominator
+            else:
+                c = c / modes.denominator
+        fine = np.zeros((rnx, rny))
+        fine[1:-1, 1:-1] = modes.inverse(c)
+        out[s] = fine[::refinement, ::refinement]
+    return out
+
+
+def level3_gates(fields: np.ndarray, standard_error: np.ndarray, params: dict,
+                 max_steps_hits: int, reference: np.ndarray | None = None,
+                 rmse_limit: float = 0.01, peak_limit: float = 0.02,
+                 statistical_argmax: bool = False) -> dict:
+    """validate_level3.py:330-420 for the fields of one run (every step):
+    per step normalised RMSE <= 1%, peak within 2% and at most one cell from
+    the reference peak; per probe the peak rise within max(5 K, 2%) and its
+    time within one step; no negative rise, no walk at the step cap.
+
+    With statistical_argmax the two argmax gates (peak cell, probe peak
+    time) fail only when the run's value at the reference's argmax lies more
+    than 3 standard errors below the run's maximum.  Where the field is flat
+    near its peak (late cooling, the 10 mm transverse probe), values a cell
+    or a few steps apart differ by less than the Monte Carlo error at 500
+    walks, so the argmax itself is noise."""
+    if reference is None:
+        reference = fd_fields_moving(params)
+    nx, ny, dt = params["nx"], params["ny"], params["dt"]
+    x = np.linspace(params["plate_x0"], params["plate_x0"] + params["length_x"], nx)
+    y = np.linspace(params["plate_y0"], params["plate_y0"] + params["length_y"], ny)
+    gate = max(x[1] - x[0], y[1] - y[0]) + 1e-12
+    failures: list[str] = []
+    if fields[:, 1:-1, 1:-1].min() < 0.0:
+        failures.append("negative interior temperature rise")
+    if max_steps_hits != 0:
+        failures.append("walks reached max_steps")
+    rows = []
+    for s in range(1, fields.shape[0]):
+        err = fields[s, 1:-1, 1:-1] - reference[s, 1:-1, 1:-1]
+        rpeak, wpeak = float(reference[s].max()), float(fields[s].max())
+        nrmse = float(np.sqrt(np.mean(err**2))) / rpeak if rpeak > 0 else 0.0
+        ri, rj = np.unravel_index(int(np.argmax(reference[s])), reference[s].shape)
+        wi, wj = np.unravel_index(int(np.argmax(fields[s])), fields[s].shape)
+        loc = float(np.hypot(x[wi] - x[ri], y[wj] - y[rj]))
+        rel = abs(wpeak - rpeak) / rpeak if rpeak > 0 else 0.0
+        rows.append({"step": s, "normalized_rmse": nrmse, "peak_relative_error": rel,
+                     "peak_location_error": loc})
+        if nrmse > rmse_limit:
+            failures.append(f"step {s}: normalized RMSE {nrmse:.3%}")
+        if rel > peak_limit:
+            failures.append(f"step {s}: peak relative error {rel:.3%}")
+        far = loc > gate
+        if far and statistical_argmax:
+            se2 = float(np.hypot(standard_error[s][wi, wj], standard_error[s][ri, rj]))
+            far = fields[s][ri, rj] < wpeak - 3.0 * se2
+        if far:
+            failures.append(f"step {s}: peak location error {loc * 1e3:.3f} mm")
+    probes = []
+    for name, px, py in LEVEL3_PROBES:
+        i, j = int(np.argmin(np.abs(x - px))), int(np.argmin(np.abs(y - py)))
+        wc, rc = fields[:, i, j], reference[:, i, j]
+        wf, rf = int(np.argmax(wc)), int(np.argmax(rc))
+        perr = float(wc[wf] - rc[rf])
+        terr = (wf - rf) * dt
+        probes.append({"probe": name, "peak_error": perr, "peak_time_error": terr})
+        if abs(perr) > max(5.0, 0.02 * float(rc[rf])):
+            failures.append(f"{name}: probe peak error {perr:.3f} K")
+        late = abs(terr) > dt + 1e-12
+        if late and statistical_argmax:
+            se2 = float(np.hypot(standard_error[wf, i, j], standard_error[rf, i, j]))
+            late = wc[rf] < wc[wf] - 3.0 * se2
+        if late:
+            failures.append(f"{name}: probe peak-time error {terr:.3f} s")
+    return {"rows": rows, "probes": probes, "failures": failures, "passed": not failures}
