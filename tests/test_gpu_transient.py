@@ -158,3 +158,28 @@ def test_fast_passes_the_reference_level3_validation(solver):
                          statistical_argmax=True)
         assert g["passed"], (seed, g["failures"][:5])
         assert max(row["normalized_rmse"] for row in g["rows"]) < 0.01
+
+
+def test_fast_level0_matches_the_discrete_cooling_solution(solver):
+    # the level-0 program's own check (apps/welding/src/level0_cooling.cpp:
+    # 286-288, 394-400): after s implicit steps the field is
+    # d^s sin(pi x) sin(pi y), d = 1 / (1 + 2 pi^2 kappa dt).  The walks
+    # sample the previous field by bilinear interpolation of its grid values;
+    # for this eigenfunction the interpolant averages (pi h)^2 / 12 below the
+    # function per axis, so each step also scales the amplitude by
+    # 1 - (pi h)^2 / 6 (0.64% on the 17 x 17 grid; the reference's own run in
+    # tests/golden is 2.7% low at the centre after five steps).  At 20 000
+    # walks FAST_FP32 must follow (d (1 - (pi h)^2 / 6))^s within 1% at the
+    # centre and 2% RMS at every step.
+    from walk_on_spheres_b200.transient import LEVEL0, level0_initial, solve_transient
+    n = LEVEL0["nx"]
+    init = level0_initial(n, n)
+    r = solve_transient(solver, method="fast", initial=init, **dict(LEVEL0, walks=20000))
+    d = 1.0 / (1.0 + 2.0 * math.pi**2 * LEVEL0["conductivity"] * LEVEL0["dt"])
+    h = 1.0 / (n - 1)
+    per_step = d * (1.0 - (math.pi * h) ** 2 / 6.0)
+    for s in range(1, r.fields.shape[0]):
+        amp = per_step**s
+        err = (r.fields[s] - amp * init)[1:-1, 1:-1]
+        assert np.sqrt(np.mean(err**2)) / amp < 0.02, (s, np.sqrt(np.mean(err**2)) / amp)
+        assert abs(r.fields[s][n // 2, n // 2] / amp - 1.0) < 0.01, (s, r.fields[s][n // 2, n // 2] / amp)
