@@ -103,3 +103,30 @@ def test_fd_reference_heats_then_cools():
     energy = sum(absorbed * heating_fraction((s - 1) * p["dt"], s * p["dt"], p["heat_on_time"])
                  * p["dt"] for s in range(1, steps + 1))
     assert abs(energy - absorbed * p["heat_on_time"]) < 1e-9
+
+
+def test_fd_moving_reference_follows_the_source():
+    # level-3 configuration: while the source is on, the FD peak rides on the
+    # weld line behind the source centre x(t) = -0.05 + 0.02 t and advances
+    # with it; after switch-off (5 s) the peak falls every step
+    from oracle.fd_transient import fd_fields_moving
+    from walk_on_spheres_b200.transient import LEVEL3
+    p = dict(defaults())
+    p.update(LEVEL3)
+    f = fd_fields_moving(p, refinement=2, substeps=4)
+    x = np.linspace(p["plate_x0"], p["plate_x0"] + p["length_x"], p["nx"])
+    y = np.linspace(p["plate_y0"], p["plate_y0"] + p["length_y"], p["ny"])
+    peak_x = []
+    for s in (10, 25, 40):
+        i, j = np.unravel_index(int(np.argmax(f[s])), f[s].shape)
+        centre = p["source_start_x"] + p["weld_speed"] * s * p["dt"]
+        assert abs(y[j] - p["weld_y"]) < 1e-12
+        assert centre - 0.02 <= x[i] <= centre + 1e-12, (s, x[i], centre)
+        peak_x.append(x[i])
+    # 3 s apart the source moves 60 mm; the peak follows, its lag growing as
+    # the thermal wake builds up (9 mm at 1 s, 12.5 mm at 2.5 s)
+    assert 0.8 * 0.06 <= peak_x[2] - peak_x[0] <= 0.06 + (x[1] - x[0]), peak_x
+    on = int(round(p["heat_on_time"] / p["dt"]))
+    peaks = f[on + 1:].max(axis=(1, 2))
+    assert np.all(np.diff(peaks) < 0.0)
+    assert np.all(f[:, 0, :] == 0.0) and np.all(f[:, :, 0] == 0.0)
