@@ -205,8 +205,9 @@ struct WideBuilder {
 }  // namespace
 
 // Principal plane of a point set: unit normal along the smallest-variance
-// direction (Jacobi eigen-decomposition of the covariance), offset n.mean and
-// half-thickness max |n.v - offset|.
+// direction (cyclic Jacobi eigen-decomposition of the covariance, rotations
+// from their tangents), offset n.mean and half-thickness max |n.v - offset|.
+// Any unit normal gives a valid slab; the thickness is measured for it.
 static void slab_of(const std::vector<double> &pts, int dim, double *n, double &c, double &h) {
     const size_t m = pts.size() / dim;
     double mean[3] = {0, 0, 0};
@@ -227,8 +228,16 @@ static void slab_of(const std::vector<double> &pts, int dim, double *n, double &
         for (int a = 0; a < dim; ++a) {
             for (int b = a + 1; b < dim; ++b) {
                 if (std::fabs(A[a][b]) < 1e-300) continue;
-                const double theta = 0.5 * std::atan2(2 * A[a][b], A[b][b] - A[a][a]);
-                const double cs = std::cos(theta), sn = std::sin(theta);
+                // the rotation that zeroes A[a][b], from its tangent
+                // (t = tan phi, |phi| <= pi/4): +, -, *, / and sqrt only, so
+                // every IEEE machine rounds it the same way
+                const double theta = (A[b][b] - A[a][a]) / (2.0 * A[a][b]);
+                const double t =
+                    std::fabs(theta) > 1e150
+                        ? 0.5 / theta
+                        : (theta >= 0.0 ? 1.0 : -1.0) /
+                              (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
                 for (int k = 0; k < dim; ++k) {  // A <- A J
                     const double x = A[k][a], y = A[k][b];
                     A[k][a] = cs * x - sn * y;
