@@ -1,5 +1,5 @@
 """Finite-difference reference of the stationary Gaussian plate problem and the
-reference's level-1 validation gates.  TEST INFRASTRUCTURE ONLY: the checker
+reference's level-1 validation gates.  TEST INFRASTRUCTURE ONLY: the oracle
 of the stationary plate solver, never part of the product path.
 
 Restates apps/welding/tools/validate_level1.py:21-187: the 5-point negative

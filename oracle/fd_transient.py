@@ -1,6 +1,6 @@
 """Finite-difference references of the transient plate problems (welding
 levels 2 and 3) and the reference's validation gates.  TEST INFRASTRUCTURE
-ONLY: the checker of the transient solver, never part of the product path.
+ONLY: the oracle of the transient solver, never part of the product path.
 
 Level 3 (moving source): fd_fields_moving / level3_gates restate
 apps/welding/tools/validate_level3.py:133-420 (below).

@@ -1,4 +1,4 @@
-"""ctypes bindings for the two CPU checkers.  TEST INFRASTRUCTURE ONLY.
+"""ctypes bindings for the two CPU oracles.  TEST INFRASTRUCTURE ONLY.
 
 * :class:`Reference` — ``oracle/_ref/libwos_ref.so``: the reference's own
   sources compiled where they lie (oracle/Makefile) plus the thin C entry
@@ -129,7 +129,7 @@ class _Lib:
                 pb.points, pb.n_points = _ptr(pts), pts.shape[0]
         return pb, keep
 
-    # ---- entry points shared by both checkers
+    # ---- entry points shared by both oracles
     def solve_grid(self, equation: str, solve: Solve) -> GridResult:
         pb, keep = self._problem(solve.mesh, solve)
         n = pb.Nx * pb.Ny * pb.Nz

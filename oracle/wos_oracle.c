@@ -1,6 +1,6 @@
 /*
  * wos_oracle.c — plain C, FP64 restatement of the reference walk-on-spheres
- * hot path.  TEST INFRASTRUCTURE ONLY (see wos_oracle.h): the checker, never
+ * hot path.  TEST INFRASTRUCTURE ONLY (see wos_oracle.h): the oracle, never
  * the product.  Compiled with -ffp-contract=off so every expression rounds
  * like the reference's C++17 build on x86-64 (no FMA contraction).
  *

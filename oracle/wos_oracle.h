@@ -1,6 +1,6 @@
 /*
  * wos_oracle — plain C, FP64 restatement of the reference walk-on-spheres hot
- * path.  TEST INFRASTRUCTURE ONLY: the checker for the CUDA library, used by
+ * path.  TEST INFRASTRUCTURE ONLY: the oracle for the CUDA library, used by
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg.  It is
  * never linked into, or called by, the product library.
  *
