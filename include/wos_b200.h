@@ -521,6 +521,58 @@ int wos_write_hdf5(const char *path, const wos_grid *grid, const double *mean,
                    long long indeterminate_points, uint64_t seed, int write_source_metadata,
                    double alpha, int source_mode);
 
+/* Parallel write path: the reference's collective hyperslab writes
+ * (include/wos/hdf5_io.hpp:51-171: every rank writes its own block of the
+ * five fields, rank 0 writes /x /y /z and the /metadata scalars) without
+ * MPI-IO.  The file layout depends only on the grid shape and the two
+ * metadata switches, so every rank can compute it (wos_hdf5_layout).
+ * One process creates the file (wos_hdf5_create): coordinates and metadata
+ * written, the five fields' storage reserved.  Then every rank writes its
+ * part of the fields into that storage (wos_hdf5_write_block or
+ * wos_hdf5_write_range). Writes to disjoint parts may run from many
+ * processes at once. Once every point has been written, the file is
+ * byte-identical to wos_write_hdf5 of the whole fields. */
+typedef struct {
+    /* file offsets of the raw values of mean, variance, standard_error,
+     * mean_steps (f64, C order) and location (u8, C order) */
+    long long field_offset[5];
+    long long file_size;
+} wos_h5_layout;
+
+/* The layout of a result file for `grid`, writing nothing. */
+int wos_hdf5_layout(const wos_grid *grid, int write_ray_metadata, int write_source_metadata,
+                    wos_h5_layout *layout);
+
+/* Create the result file with every dataset but the fields' values
+ * (arguments as wos_write_hdf5); `layout` (may be null) receives its layout.
+ * The metadata counters are the totals over all ranks (the reference reduces
+ * them first, include/wos/runner.hpp:240-263). */
+int wos_hdf5_create(const char *path, const wos_grid *grid, int N_walks, double epsilon,
+                    int max_steps, long long max_steps_hits, int write_ray_metadata,
+                    int max_ray_attempts, long long ambiguous_ray_retries,
+                    long long indeterminate_points, uint64_t seed, int write_source_metadata,
+                    double alpha, int source_mode, wos_h5_layout *layout);
+
+/* Write one rank's block of the fields into a created file: grid points
+ * offset[d] .. offset[d] + count[d] - 1 along x, y, z (the reference's
+ * x_start / block_Nx etc., include/wos/runner.hpp:116-128).  The arrays hold
+ * the block in C order, count[0] x count[1] x count[2] values, like the
+ * reference's per-rank Field3D.  WOS_ERR_INVALID if the block leaves the
+ * grid; WOS_ERR_IO if the file is missing, is not a result file with this
+ * layout, or a write fails. */
+int wos_hdf5_write_block(const char *path, const wos_h5_layout *layout, const wos_grid *grid,
+                         const int offset[3], const int count[3], const double *mean,
+                         const double *variance, const double *standard_error,
+                         const double *mean_steps, const uint8_t *location);
+
+/* Write grid points start .. start + count - 1 in linear (C) order, the shard
+ * of a linear-index split; the arrays hold `count` values.  Errors as
+ * wos_hdf5_write_block. */
+int wos_hdf5_write_range(const char *path, const wos_h5_layout *layout, const wos_grid *grid,
+                         long long start, long long count, const double *mean,
+                         const double *variance, const double *standard_error,
+                         const double *mean_steps, const uint8_t *location);
+
 /* Peek the mesh dimension (2 if the first primitive record is `l`, 3 if `f`),
  * src/mesh.cpp:51-74.  Returns 2, 3, or 0 on error. */
 int wos_peek_mesh_dim(const char *path);

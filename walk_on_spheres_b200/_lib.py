@@ -87,6 +87,11 @@ class StationaryParams(C.Structure):
                 ("max_proposal_attempts", C.c_int)]
 
 
+class H5Layout(C.Structure):
+    """wos_h5_layout: file offsets of the five fields' values, and the file size."""
+    _fields_ = [("field_offset", C.c_longlong * 5), ("file_size", C.c_longlong)]
+
+
 RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
                      C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double,
                      C.c_int)
@@ -146,6 +151,19 @@ SIGNATURES = {
     "wos_build_wide_bvh": (C.c_int, [C.c_int, VP, C.c_int, VP, C.c_int] + [VP] * 5),
     "wos_equation_registry": (C.POINTER(EquationEntry), [C.POINTER(C.c_int)]),
     "wos_peek_mesh_dim": (C.c_int, [C.c_char_p]),
+    # result files: serial writer and the parallel path (create, then blocks)
+    "wos_write_hdf5": (C.c_int, [C.c_char_p, C.POINTER(Grid)] + [VP] * 5 + [
+        C.c_int, C.c_double, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_longlong,
+        C.c_longlong, C.c_uint64, C.c_int, C.c_double, C.c_int]),
+    "wos_hdf5_layout": (C.c_int, [C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(H5Layout)]),
+    "wos_hdf5_create": (C.c_int, [C.c_char_p, C.POINTER(Grid), C.c_int, C.c_double, C.c_int,
+                                  C.c_longlong, C.c_int, C.c_int, C.c_longlong, C.c_longlong,
+                                  C.c_uint64, C.c_int, C.c_double, C.c_int,
+                                  C.POINTER(H5Layout)]),
+    "wos_hdf5_write_block": (C.c_int, [C.c_char_p, C.POINTER(H5Layout), C.POINTER(Grid),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)] + [VP] * 5),
+    "wos_hdf5_write_range": (C.c_int, [C.c_char_p, C.POINTER(H5Layout), C.POINTER(Grid),
+                                       C.c_longlong, C.c_longlong] + [VP] * 5),
 }
 
 _lib = None

@@ -26,9 +26,33 @@ constexpr int kLeafK = 16;
 constexpr int kInternalK = 16;
 constexpr uint64_t kUndef = ~0ull;
 
+// File image under construction: `b` holds the bytes from file offset `base`
+// on; hole(n) closes that segment and leaves n bytes unwritten, storage that
+// other writers fill in later (a POSIX file reads zeros there until then).
 struct Buf {
     std::vector<uint8_t> b;
-    size_t tell() const { return b.size(); }
+    uint64_t base = 0;
+    std::vector<std::pair<uint64_t, std::vector<uint8_t>>> done;  // closed segments
+    uint64_t tell() const { return base + b.size(); }
+    void hole(uint64_t n) {
+        const uint64_t end = tell();
+        if (!b.empty()) done.emplace_back(base, std::move(b));
+        b.clear();
+        base = end + n;
+    }
+    // overwrite n bytes at file offset `at` (inside a written segment)
+    bool patch(uint64_t at, const uint8_t *p, size_t n) {
+        auto fits = [&](uint64_t off, std::vector<uint8_t> &v) {
+            if (at < off || at + n > off + v.size()) return false;
+            std::memcpy(v.data() + (at - off), p, n);
+            return true;
+        };
+        if (fits(base, b)) return true;
+        for (auto &seg : done) {
+            if (fits(seg.first, seg.second)) return true;
+        }
+        return false;
+    }
     void u8(uint8_t v) { b.push_back(v); }
     void u16(uint16_t v) { for (int i = 0; i < 2; ++i) b.push_back(static_cast<uint8_t>(v >> (8 * i))); }
     void u32(uint32_t v) { for (int i = 0; i < 4; ++i) b.push_back(static_cast<uint8_t>(v >> (8 * i))); }
@@ -38,8 +62,7 @@ struct Buf {
         b.insert(b.end(), q, q + n);
     }
     void zeros(size_t n) { b.insert(b.end(), n, 0); }
-    void align8() { while (b.size() % 8) b.push_back(0); }
-    void put_u64(size_t at, uint64_t v) { for (int i = 0; i < 8; ++i) b[at + i] = static_cast<uint8_t>(v >> (8 * i)); }
+    void align8() { while (tell() % 8) b.push_back(0); }
 };
 
 size_t elem_size(H5Type t) {
@@ -103,14 +126,22 @@ void object_header(Buf &o, const std::vector<std::pair<uint16_t, std::vector<uin
     for (size_t i = 0; i < msgs.size(); ++i) message(o, msgs[i].first, msgs[i].second, flags[i]);
 }
 
-// Writes a dataset; returns its object header address.
+// Writes a dataset (its raw data first, then its object header); returns the
+// object header address.  Without data the raw data's storage is a hole.
 uint64_t emit_dataset(Buf &o, const H5Dataset &d) {
     uint64_t n = 1;
     for (uint64_t v : d.dims) n *= v;
     const size_t nbytes = static_cast<size_t>(n) * elem_size(d.type);
     o.align8();
     const uint64_t data_addr = o.tell();
-    if (nbytes) o.bytes(d.data, nbytes);
+    if (d.data_addr) *d.data_addr = data_addr;
+    if (nbytes) {
+        if (d.data) {
+            o.bytes(d.data, nbytes);
+        } else {
+            o.hole(nbytes);
+        }
+    }
     o.align8();
     const uint64_t hdr = o.tell();
 
@@ -230,9 +261,9 @@ GroupAddrs emit_group(Buf &o, const H5Group &g) {
 
 }  // namespace
 
-std::string write_h5(const std::string &path, const H5Group &root) {
+namespace {
+std::string build_h5(const H5Group &root, Buf &o) {
     if (root.datasets.size() + root.groups.size() > 2 * kLeafK) return "too many links in one group";
-    Buf o;
     o.zeros(96);  // superblock, filled below
     const GroupAddrs r = emit_group(o, root);
     Buf sb;
@@ -259,13 +290,42 @@ std::string write_h5(const std::string &path, const H5Group &root) {
     sb.u32(0);
     sb.u64(r.btree);
     sb.u64(r.heap);
-    std::memcpy(o.b.data(), sb.b.data(), 96);
+    if (!o.patch(0, sb.b.data(), 96)) return "superblock outside the written image";
+    return std::string();
+}
+}  // namespace
 
+std::string layout_h5(const H5Group &root, uint64_t *file_size) {
+    Buf o;
+    const std::string err = build_h5(root, o);
+    if (err.empty() && file_size) *file_size = o.tell();
+    return err;
+}
+
+std::string write_h5(const std::string &path, const H5Group &root, uint64_t *file_size) {
+    Buf o;
+    std::string err = build_h5(root, o);
+    if (!err.empty()) return err;
+    const uint64_t eof = o.tell();
+    o.hole(0);  // close the last segment
     FILE *f = std::fopen(path.c_str(), "wb");
     if (!f) return "could not create " + path;
-    const size_t w = std::fwrite(o.b.data(), 1, o.b.size(), f);
+    bool ok = true;
+    uint64_t at = 0;  // end of the bytes written so far
+    for (const auto &seg : o.done) {
+        ok = ok && fseeko(f, static_cast<off_t>(seg.first), SEEK_SET) == 0 &&
+             std::fwrite(seg.second.data(), 1, seg.second.size(), f) == seg.second.size();
+        at = seg.first + seg.second.size();
+    }
+    if (ok && at < eof) {
+        // the image ends in a hole: extend the file to its full size
+        const uint8_t zero = 0;
+        ok = fseeko(f, static_cast<off_t>(eof - 1), SEEK_SET) == 0 &&
+             std::fwrite(&zero, 1, 1, f) == 1;
+    }
     const int c = std::fclose(f);
-    if (w != o.b.size() || c != 0) return "could not write " + path;
+    if (!ok || c != 0) return "could not write " + path;
+    if (file_size) *file_size = eof;
     return std::string();
 }
 

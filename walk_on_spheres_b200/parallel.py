@@ -5,10 +5,13 @@ because every point is seeded from its global linear index
 (runner.hpp:163-168) the fields do not depend on the split (README.md:87-90).
 Here rank r solves the contiguous linear-index range
 [n*r/world, n*(r+1)/world) of the grid — its own points, seeded by their
-global index — and rank 0 gathers the fields and sums the counters, the
-counterpart of runner.hpp:240-263 and of the collective HDF5 write.  There
-is no collective inside the walk loop; the only communication is one gather
-of the fields and one reduction of a few scalars at the end.
+global index.  Either rank 0 gathers the fields and sums the counters
+(solve_grid_sharded, the counterpart of runner.hpp:240-263), or every rank
+writes its range straight into the result file after rank 0 creates it
+(solve_grid_sharded_to_file, the counterpart of the collective HDF5 write,
+include/wos/hdf5_io.hpp:51-171).  There is no collective inside the walk
+loop; the only communication is a reduction of a few scalars at the end, and
+the gather or two barriers.
 
     import torch.distributed as dist
     from walk_on_spheres_b200 import Solver, meshes, parallel
@@ -114,3 +117,64 @@ def solve_grid_sharded(solve_shard, n_points: int, group=None, device=None) -> d
     out["counters"] = {k: int(v) for k, v in zip(COUNTS, counts.cpu().tolist())}
     out["counters"]["total_ms_max_over_ranks"] = float(times.item())
     return out
+
+
+def solve_grid_sharded_to_file(solve_shard, grid, path, meta, group=None,
+                               device=None) -> dict:
+    """Solve this rank's shard and write it straight into the result file at
+    `path`: the reference's parallel HDF5 write (include/wos/hdf5_io.hpp:51-171),
+    with no gather of the fields.  The counters are summed over the ranks
+    first, as runner.hpp:240-263 does, and rank 0 creates the file with them in
+    /metadata (`meta` gives the run settings; its counters are replaced).
+    Then every rank writes its own linear-index range.  Every rank takes the
+    same collective steps on failure too: a failed create or write raises on
+    all ranks.  Returns the summed counters on every rank."""
+    import dataclasses
+
+    import torch
+    import torch.distributed as dist
+
+    from . import results
+
+    rank = dist.get_rank(group)
+    world = dist.get_world_size(group)
+    n_points = int(grid.Nx) * int(grid.Ny) * int(grid.Nz)
+    start, end = shard_bounds(n_points, rank, world)
+    local = solve_shard(start, end)
+    c = local.get("counters", {})
+    counts = torch.tensor([float(c.get(k, 0)) for k in COUNTS], dtype=torch.float64)
+    times = torch.tensor([float(c.get("total_ms", 0.0))], dtype=torch.float64)
+    on_device = device is not None and str(device) != "cpu"
+    if on_device:
+        counts, times = counts.to(device), times.to(device)
+    dist.all_reduce(counts, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(times, op=dist.ReduceOp.MAX, group=group)
+    total = {k: int(v) for k, v in zip(COUNTS, counts.cpu().tolist())}
+    total["total_ms_max_over_ranks"] = float(times.item())
+
+    def agree(ok: bool, what: str):
+        flag = torch.tensor([1 if ok else 0], dtype=torch.int32)
+        if on_device:
+            flag = flag.to(device)
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN, group=group)
+        if int(flag.item()) == 0:
+            raise RuntimeError(f"sharded HDF5 write: {what} failed on a rank")
+
+    error = None
+    if rank == 0:
+        full = dataclasses.replace(meta, max_steps_hits=total["max_steps_hits"],
+                                   ambiguous_ray_retries=total["ambiguous_ray_retries"],
+                                   indeterminate_points=total["indeterminate_points"])
+        try:
+            results.create(path, grid, full)
+        except (RuntimeError, OSError) as e:
+            error = e
+    agree(error is None, "creating the file")
+    try:
+        lay = results.layout(grid, meta.write_ray_metadata, meta.write_source_metadata)
+        results.write_range(path, lay, grid, start,
+                            {k: np.asarray(local[k])[:end - start] for k in FIELDS})
+    except (RuntimeError, OSError, ValueError) as e:
+        error = e
+    agree(error is None, "writing a shard")
+    return total
