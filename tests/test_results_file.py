@@ -228,3 +228,42 @@ def test_two_ranks_write_the_single_process_file(tmp_path, oracle, name):
     want = _serial_bytes(tmp_path, _grid_over(mesh, shape),
                          {k: getattr(ref, k) for k in results.FIELDS}, full)
     assert open(path, "rb").read() == want
+
+
+def _failing_worker(rank, world, port, path, results_q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        grid = _grid(4, 3, 1)
+
+        def solve(start, end):
+            f = _fields(end - start, start)
+            f["counters"] = {"inside_points": end - start}
+            return f
+
+        try:
+            parallel.solve_grid_sharded_to_file(solve, grid, path, META2)
+            results_q.put((rank, "no error"))
+        except RuntimeError as e:
+            results_q.put((rank, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_failed_create_raises_on_every_rank(tmp_path):
+    """Rank 0 cannot create the file (its directory does not exist): every
+    rank raises after the same collective steps instead of waiting."""
+    path = str(tmp_path / "no_such_dir" / "r.h5")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, path, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all("creating the file failed" in got[r] for r in range(2)), got
