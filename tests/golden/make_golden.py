@@ -40,6 +40,18 @@ GRID_CASES = [
     ("sphere_poisson", "poisson", "sphere", (7, 7, 7), 100, 11, {"source_mode": 1}),
     ("sphere_screened", "screened_poisson", "sphere", (8, 8, 8), 100, 7, {"alpha": 10.0}),
     ("sphere_helmholtz", "helmholtz", "sphere", (7, 7, 7), 100, 2, {}),
+    # edge cases: walks cut at max_steps (value g at the last nearest point,
+    # counted in max_steps_hits), one walk per point (variance 0), a grid row
+    # (Ny = 1: y = ymin, one point on the boundary), a wide epsilon shell, the
+    # 3D classification with its minimum of three rays
+    ("annulus_laplace_max_steps", "laplace", "annulus", (10, 10, 1), 60, 21, {"max_steps": 3}),
+    ("sphere_laplace_max_steps", "laplace", "sphere", (5, 5, 5), 30, 17, {"max_steps": 2}),
+    ("circle_poisson_one_walk", "poisson", "circle256", (9, 9, 1), 1, 4, {"source_mode": 1}),
+    ("annulus_laplace_row", "laplace", "annulus", (17, 1, 1), 50, 8, {}),
+    ("circle_helmholtz_wide_shell", "helmholtz", "circle256", (10, 10, 1), 100, 6,
+     {"epsilon": 0.2}),
+    ("sphere_poisson_three_rays", "poisson", "sphere", (6, 6, 6), 40, 13,
+     {"max_ray_attempts": 3, "source_mode": 0}),
 ]
 
 

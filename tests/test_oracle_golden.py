@@ -121,6 +121,10 @@ def test_grid_solves(oracle, golden, case):
             assert np.array_equal(got, want), k
         else:
             assert np.allclose(got, want, rtol=1e-12, atol=1e-15), k
+    # boundary points carry g at the point itself, outside points NaN
+    bnd = res.location == 2
+    assert np.array_equal(res.mean[bnd], golden[pre + "mean"][bnd])
+    assert np.isnan(res.mean[(res.location == 0) | (res.location == 3)]).all()
     c = golden[pre + "counters"]
     assert res.counters["inside_points"] == c[0]
     assert res.counters["max_steps_hits"] == c[1]
