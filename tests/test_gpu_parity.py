@@ -169,3 +169,34 @@ def test_sharded_solver_matches_grid(solver):
     assert np.array_equal(out["location"], g.location.ravel())
     ins = out["location"] == 1
     assert np.allclose(out["mean"][ins], g.mean.ravel()[ins], rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("method", ["fast", "fast64"])
+def test_fast_edge_cases(solver, golden, method):
+    """The FAST methods on the reference's edge cases: a grid row with no
+    inside point (nothing to walk, boundary values exact), one walk per point
+    (variance 0, as the reference defines it), and walks cut at max_steps
+    (hits counted, no walk longer than the cap)."""
+    by = {c[0]: c for c in GRID_CASES}
+    pre = "grid_annulus_laplace_row_"
+    r = _solve(solver, by["annulus_laplace_row"], method)
+    loc = golden[pre + "location"].reshape(r.location.shape)
+    assert np.array_equal(r.location, loc)
+    assert r.counters["inside_points"] == 0 and r.counters["total_walks"] == 0
+    bnd = loc == 2
+    assert bnd.any()
+    assert np.allclose(r.mean[bnd], golden[pre + "mean"].reshape(loc.shape)[bnd],
+                       rtol=1e-13, atol=1e-15)
+    assert np.isnan(r.mean[loc == 0]).all()
+
+    r = _solve(solver, by["circle_poisson_one_walk"], method)
+    ins = r.location == 1
+    assert ins.sum() == golden["grid_circle_poisson_one_walk_counters"][0]
+    assert np.all(r.variance[ins] == 0.0) and np.all(r.standard_error[ins] == 0.0)
+    assert np.all(np.isfinite(r.mean[ins]))
+
+    for name, cap in (("annulus_laplace_max_steps", 3), ("sphere_laplace_max_steps", 2)):
+        r = _solve(solver, by[name], method)
+        ins = r.location == 1
+        assert r.counters["max_steps_hits"] > 0
+        assert np.all(r.mean_steps[ins] <= cap) and np.all(np.isfinite(r.mean[ins]))
