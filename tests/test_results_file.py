@@ -267,3 +267,9 @@ def test_failed_create_raises_on_every_rank(tmp_path):
         p.join(timeout=60)
         assert p.exitcode == 0
     assert all("creating the file failed" in got[r] for r in range(2)), got
+
+
+def test_serial_write_error_is_reported(tmp_path):
+    grid = _grid(2, 2, 1)
+    with pytest.raises(RuntimeError, match="could not create"):
+        results.write(tmp_path / "no_such_dir" / "r.h5", grid, _fields(4, 1), META2)

@@ -256,10 +256,10 @@ extern "C" int wos_write_hdf5(const char *path, const wos_grid *grid, const doub
                               long long ambiguous_ray_retries, long long indeterminate_points,
                               uint64_t seed, int write_source_metadata, double alpha,
                               int source_mode) {
-    if (!path || !mean || !variance || !standard_error || !mean_steps || !location) {
-        return WOS_ERR_INVALID;
+    if (!path || !mean || !variance || !standard_error || !mean_steps || !location ||
+        !grid_ok(grid)) {
+        return wosb::fail(nullptr, WOS_ERR_INVALID, "HDF5 write: null argument or empty grid");
     }
-    if (!grid_ok(grid)) return WOS_ERR_INVALID;
     const ResultMeta m{N_walks, epsilon, max_steps, max_steps_hits, write_ray_metadata,
                        max_ray_attempts, ambiguous_ray_retries, indeterminate_points, seed,
                        write_source_metadata, alpha, source_mode};
@@ -267,8 +267,9 @@ extern "C" int wos_write_hdf5(const char *path, const wos_grid *grid, const doub
     const ResultTree t(*grid, fields, m);
     const std::string err = wosb::write_h5(path, t.root);
     if (!err.empty()) {
-        std::fprintf(stderr, "HDF5 error while writing %s: %s\n", path, err.c_str());
-        return WOS_ERR_IO;
+        const std::string msg = std::string("HDF5 error while writing ") + path + ": " + err;
+        std::fprintf(stderr, "%s\n", msg.c_str());
+        return wosb::fail(nullptr, WOS_ERR_IO, msg);
     }
     return WOS_OK;
 }

@@ -82,7 +82,7 @@ def write(path, grid, fields: dict, meta: ResultMeta) -> None:
     rc = _lib.lib().wos_write_hdf5(str(path).encode(), C.byref(grid), *_ptrs(arrays),
                                    *meta.args())
     if rc != 0:
-        raise RuntimeError(f"wos_write_hdf5 failed (status {rc}) for {path}")
+        _error("wos_write_hdf5", rc)
 
 
 def layout(grid, write_ray_metadata: bool, write_source_metadata: bool) -> _lib.H5Layout:
