@@ -42,7 +42,10 @@ def _serial_bytes(tmp_path, grid, fields, meta):
     return p.read_bytes()
 
 
-SHAPES = [((7, 5, 1), META2), ((1, 1, 1), META2), ((6, 5, 4), META3), ((3, 1, 9), META3)]
+# the last shape's f64 fields (128 KB each) are written from the caller's
+# arrays, the smaller ones through the file image
+SHAPES = [((7, 5, 1), META2), ((1, 1, 1), META2), ((6, 5, 4), META3), ((3, 1, 9), META3),
+          ((40, 40, 10), META3)]
 
 
 @pytest.mark.parametrize("shape,meta", SHAPES)
@@ -58,6 +61,9 @@ def test_range_shards_equal_the_serial_file(tmp_path, shape, meta):
     for s, e in reversed(spans):                               # any order
         results.write_range(p, lay, grid, s, {k: v[s:e] for k, v in fields.items()})
     assert p.read_bytes() == want
+    f = h5lite.read(tmp_path / "serial.h5")
+    for k in results.FIELDS:
+        np.testing.assert_array_equal(f["/" + k].ravel(), fields[k])
 
 
 def _reference_blocks(shape, dims):

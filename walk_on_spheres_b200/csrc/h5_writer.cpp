@@ -25,20 +25,34 @@ namespace {
 constexpr int kLeafK = 16;
 constexpr int kInternalK = 16;
 constexpr uint64_t kUndef = ~0ull;
+// datasets of at least this many bytes are written from the caller's array
+constexpr size_t kExternalBytes = 1 << 16;
 
 // File image under construction: `b` holds the bytes from file offset `base`
 // on; hole(n) closes that segment and leaves n bytes unwritten, storage that
 // other writers fill in later (a POSIX file reads zeros there until then).
+// external(p, n) is a hole that the file write fills from the caller's array
+// p, so large datasets are not copied into the image.
 struct Buf {
+    struct External {
+        uint64_t at;
+        const void *p;
+        size_t n;
+    };
     std::vector<uint8_t> b;
     uint64_t base = 0;
     std::vector<std::pair<uint64_t, std::vector<uint8_t>>> done;  // closed segments
+    std::vector<External> ext;
     uint64_t tell() const { return base + b.size(); }
     void hole(uint64_t n) {
         const uint64_t end = tell();
         if (!b.empty()) done.emplace_back(base, std::move(b));
         b.clear();
         base = end + n;
+    }
+    void external(const void *p, size_t n) {
+        ext.push_back({tell(), p, n});
+        hole(n);
     }
     // overwrite n bytes at file offset `at` (inside a written segment)
     bool patch(uint64_t at, const uint8_t *p, size_t n) {
@@ -136,10 +150,12 @@ uint64_t emit_dataset(Buf &o, const H5Dataset &d) {
     const uint64_t data_addr = o.tell();
     if (d.data_addr) *d.data_addr = data_addr;
     if (nbytes) {
-        if (d.data) {
-            o.bytes(d.data, nbytes);
-        } else {
+        if (!d.data) {
             o.hole(nbytes);
+        } else if (nbytes >= kExternalBytes) {
+            o.external(d.data, nbytes);
+        } else {
+            o.bytes(d.data, nbytes);
         }
     }
     o.align8();
@@ -312,11 +328,13 @@ std::string write_h5(const std::string &path, const H5Group &root, uint64_t *fil
     if (!f) return "could not create " + path;
     bool ok = true;
     uint64_t at = 0;  // end of the bytes written so far
-    for (const auto &seg : o.done) {
-        ok = ok && fseeko(f, static_cast<off_t>(seg.first), SEEK_SET) == 0 &&
-             std::fwrite(seg.second.data(), 1, seg.second.size(), f) == seg.second.size();
-        at = seg.first + seg.second.size();
-    }
+    auto put = [&](uint64_t off, const void *p, size_t n) {
+        ok = ok && fseeko(f, static_cast<off_t>(off), SEEK_SET) == 0 &&
+             std::fwrite(p, 1, n, f) == n;
+        at = std::max(at, off + n);
+    };
+    for (const auto &seg : o.done) put(seg.first, seg.second.data(), seg.second.size());
+    for (const Buf::External &e : o.ext) put(e.at, e.p, e.n);
     if (ok && at < eof) {
         // the image ends in a hole: extend the file to its full size
         const uint8_t zero = 0;
