@@ -279,3 +279,61 @@ def test_serial_write_error_is_reported(tmp_path):
     grid = _grid(2, 2, 1)
     with pytest.raises(RuntimeError, match="could not create"):
         results.write(tmp_path / "no_such_dir" / "r.h5", grid, _fields(4, 1), META2)
+
+
+# --------------------------------------------- a registry run's metadata
+
+RUNS = [("laplace", "annulus", (9, 8, 1), 40, 1e-2, 3, 5.0, 0),
+        ("poisson", "circle", (8, 8, 1), 40, 2e-2, 4, 5.0, 1),
+        ("screened_poisson", "sphere", (5, 5, 5), 20, 1e-2, 7, 10.0, 0),
+        ("helmholtz", "sphere", (5, 4, 5), 20, 1e-2, 9, 5.0, 0)]
+
+
+@pytest.mark.parametrize("run", RUNS, ids=[r[0] for r in RUNS])
+def test_writer_reproduces_reference_registry_file(tmp_path, reference, run):
+    """Our writer, given a reference registry run's fields and the metadata
+    rules of results.run_meta, writes exactly the datasets that run wrote."""
+    eq, mname, shape, walks, eps, seed, alpha, mode = run
+    mesh = {"annulus": meshes.annulus(segments=32), "circle": meshes.circle(segments=64),
+            "sphere": meshes.uv_sphere(lon=12, lat=6)}[mname]
+    obj = meshes.write_obj(mesh, tmp_path / "m.obj")
+    ref = reference.run_registry(eq, mesh.dim, str(obj), *shape, walks, eps, 1000, 12, seed,
+                                 alpha, mode)
+    eff = min(eps, 0.05 / alpha) if eq == "screened_poisson" else eps
+    counters = {k: int(ref["/metadata/" + k].view(np.int64)[0])
+                for k in ("max_steps_hits", "ambiguous_ray_retries", "indeterminate_points")
+                if "/metadata/" + k in ref}
+    meta = results.run_meta(eq, mesh.dim, walks, eff, 1000, seed, alpha=alpha, source_mode=mode,
+                            max_ray_attempts=12, counters=counters)
+    x, y, z = (ref[a].view(np.float64) for a in ("/x", "/y", "/z"))
+    grid = _lib.Grid(*shape, x[0], x[-1], y[0], y[-1], z[0], z[-1])
+    fields = {k: ref["/" + k].view(np.uint8 if k == "location" else np.float64)
+              for k in results.FIELDS}
+    results.write(tmp_path / "ours.h5", grid, fields, meta)
+    ours = h5lite.read(tmp_path / "ours.h5")
+    assert set(ours) == set(ref)
+    for name, raw in ref.items():
+        assert ours[name].tobytes() == raw.tobytes(), name
+
+
+def test_grid_result_writes_its_run(tmp_path):
+    """GridResult.write_hdf5 (a Solver.solve_grid result) writes the file of
+    results.run_meta for its equation, parameters and counters."""
+    from walk_on_spheres_b200.solver import GridResult
+    grid = _grid(4, 3, 2)
+    f = _fields(24, 3)
+    p = _lib.Params(2, 1, 10.0, 64, 1e-2, 1000, 12, 77, 1)      # screened_poisson, Green
+    c = {"max_steps_hits": 2, "ambiguous_ray_retries": 5, "indeterminate_points": 1,
+         "effective_epsilon": 0.005}
+    r = GridResult(*[f[k].reshape(4, 3, 2) for k in results.FIELDS], counters=c,
+                   equation="screened_poisson", dim=3, grid=grid, params=p)
+    r.write_hdf5(tmp_path / "r.h5")
+    want = results.run_meta("screened_poisson", 3, 64, 0.005, 1000, 77, alpha=10.0,
+                            source_mode=1, counters=c)
+    results.write(tmp_path / "w.h5", grid, f, want)
+    assert (tmp_path / "r.h5").read_bytes() == (tmp_path / "w.h5").read_bytes()
+    m = h5lite.read(tmp_path / "r.h5")
+    assert m["/metadata/epsilon"] == 0.005 and m["/metadata/alpha"] == 10.0
+    assert m["/metadata/ambiguous_ray_retries"] == 5
+    with pytest.raises(ValueError):
+        GridResult(*[f[k] for k in results.FIELDS]).write_hdf5(tmp_path / "x.h5")

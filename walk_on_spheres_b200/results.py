@@ -52,6 +52,26 @@ class ResultMeta:
                 int(bool(self.write_source_metadata)), float(self.alpha), int(self.source_mode))
 
 
+def run_meta(equation: str, dim: int, N_walks: int, effective_epsilon: float, max_steps: int,
+             seed: int, alpha: float = 0.0, source_mode: int = 0, max_ray_attempts: int = 12,
+             counters: dict | None = None) -> ResultMeta:
+    """The /metadata a registry run writes (the equation files' run calls,
+    src/equations/*.cpp): the effective epsilon (screened_poisson reduces it,
+    screened_poisson.cpp:22-38); the ray counters in 3D; alpha and
+    source_mode for poisson (alpha 0, poisson.cpp:126-134) and
+    screened_poisson only.  `counters` are the run's totals."""
+    c = counters or {}
+    source = equation in ("poisson", "screened_poisson")
+    return ResultMeta(N_walks=N_walks, epsilon=effective_epsilon, max_steps=max_steps,
+                      max_steps_hits=int(c.get("max_steps_hits", 0)),
+                      write_ray_metadata=dim == 3, max_ray_attempts=max_ray_attempts,
+                      ambiguous_ray_retries=int(c.get("ambiguous_ray_retries", 0)),
+                      indeterminate_points=int(c.get("indeterminate_points", 0)), seed=seed,
+                      write_source_metadata=source,
+                      alpha=alpha if equation == "screened_poisson" else 0.0,
+                      source_mode=int(source_mode))
+
+
 def _error(what: str, rc: int):
     msg = _lib.lib().wos_last_global_error().decode(errors="replace")
     raise RuntimeError(f"{what} failed (status {rc}): {msg}")

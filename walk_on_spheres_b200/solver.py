@@ -34,13 +34,32 @@ def _ptr(a):
 
 @dataclass
 class GridResult:
-    """Fields of one sweep in row-major (i, j, k) order, shaped (Nx, Ny, Nz)."""
+    """Fields of one sweep in row-major (i, j, k) order, shaped (Nx, Ny, Nz).
+    A grid sweep also records what it ran (`equation`, `dim`, `grid`,
+    `params`), so `write_hdf5` can write the reference's result file."""
     mean: np.ndarray
     variance: np.ndarray
     standard_error: np.ndarray
     mean_steps: np.ndarray
     location: np.ndarray
     counters: dict = field(default_factory=dict)
+    equation: str | None = None
+    dim: int = 0
+    grid: object = None
+    params: object = None
+
+    def write_hdf5(self, path) -> None:
+        """Write the result file a registry run of the same sweep writes
+        (include/wos/hdf5_io.hpp layout, the run's /metadata)."""
+        from . import results
+        if self.grid is None or self.params is None or self.equation is None:
+            raise ValueError("write_hdf5 needs a grid sweep's result (Solver.solve_grid)")
+        p = self.params
+        meta = results.run_meta(self.equation, self.dim, p.N_walks,
+                                self.counters["effective_epsilon"], p.max_steps, p.seed,
+                                alpha=p.alpha, source_mode=p.source_mode,
+                                max_ray_attempts=p.max_ray_attempts, counters=self.counters)
+        results.write(path, self.grid, {k: getattr(self, k) for k in results.FIELDS}, meta)
 
 
 def _enum(value, table, what):
@@ -150,6 +169,11 @@ class Solver:
         for k in ("mean", "variance", "standard_error", "mean_steps", "location"):
             setattr(res, k, getattr(res, k).reshape(shape))
         res.counters = c.as_dict()
+        res.equation = EQUATIONS[p.equation]
+        res.dim = self.dim
+        res.grid = _lib.Grid(g.Nx, g.Ny, shape[2], g.xmin, g.xmax, g.ymin, g.ymax,
+                             g.zmin, g.zmax)
+        res.params = p
         return res
 
     def solve_grid_device(self, equation, grid: _lib.Grid, mean=0, variance=0,
