@@ -300,3 +300,52 @@ def test_threaded_build_is_bit_identical_to_a_serial_build():
     assert serial["nodes"].size > 0 and serial["order"].size == 57120
     for k in serial:
         assert np.array_equal(serial[k], threaded[k]), k
+
+
+# OBJ dialect edge cases: whatever the reference's loader does (load, or fail
+# with a message), wos_read_obj must do the same
+EDGE_OBJS = {
+    "crlf.obj": "v 0 0\r\nv 1 0\r\nv 1 1\r\nl 1 2 3 1\r\n",
+    "tabs.obj": "v\t0\t0\nv  1   0\nv 1 1\t\nl\t1 2  3\n",
+    "leading_space.obj": "  v 0 0\n v 1 0\nv 1 1\n  l 1 2 3\n",
+    "scientific.obj": "v 1e-3 -2.5E+1\nv 1.5e0 0\nv +2 .5\nl 1 2 3\n",
+    "no_final_newline.obj": "v 0 0\nv 1 0\nv 1 1\nl 1 2 3",
+    "blank_lines.obj": "\n\nv 0 0\n   \nv 1 0\nv 1 1\n\nl 1 2 3\n\n",
+    "negative_index.obj": "v 0 0\nv 1 0\nv 1 1\nl -3 -2 -1\n",
+    "other_records.obj": "mtllib a.mtl\no obj\ng grp\nv 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\n"
+                         "vn 0 0 1\nvt 0 0\ns off\nusemtl m\nf 1 3 2\nf 1 2 4\nf 2 3 4\nf 1 4 3\n",
+    "face_slashes.obj": "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf 1/1/1 3//3 2/2\nf 1 2 4\n"
+                        "f 2 3 4\nf 1 4 3\n",
+    "line_in_3d.obj": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\nl 1 2\n",
+    "face_in_2d.obj": "v 0 0\nv 1 0\nv 1 1\nl 1 2 3\nf 1 2 3\n",
+    "vertex_w.obj": "v 0 0 0 1\nv 1 0 0 1\nv 0 1 0 1\nv 0 0 1 1\nf 1 3 2\nf 1 2 4\n"
+                    "f 2 3 4\nf 1 4 3\n",
+    "z_in_2d.obj": "v 0 0 0\nv 1 0 0\nv 1 1 0\nl 1 2 3\n",
+    "two_loops_closed.obj": "v 0 0\nv 4 0\nv 4 4\nv 0 4\nl 1 2 3 4 1\nv 1 1\nv 2 1\nv 2 2\n"
+                            "l 5 6 7 5\n",
+    "comment_only_line.obj": "# header\n#\nv 0 0 # a\nv 1 0\nv 1 1\nl 1 2 3 # closing\n",
+    "uppercase_record.obj": "V 0 0\nV 1 0\nV 1 1\nL 1 2 3\n",
+    "long_polyline.obj": "".join(f"v {np.cos(t):.17g} {np.sin(t):.17g}\n"
+                                 for t in np.linspace(0, 2 * np.pi, 200, endpoint=False))
+                         + "l " + " ".join(str(i) for i in range(1, 201)) + " 1\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(EDGE_OBJS))
+def test_obj_edge_cases_match_reference(tmp_path, reference, name):
+    p = tmp_path / name
+    p.write_bytes(EDGE_OBJS[name].encode())
+    rc, got = read_obj(p)
+    try:
+        rdim, rv, rp, rb = reference.load_mesh(str(p))
+    except ValueError as e:
+        assert rc == 3, f"reference rejects ({e}); ours loads"
+        assert got == str(e)
+        return
+    assert rc == 0, f"reference loads; ours rejects: {got}"
+    dim, verts, prims, bids = got
+    assert dim == rdim
+    assert np.array_equal(verts, rv)
+    assert np.array_equal(prims, rp)
+    if dim == 2:
+        assert np.array_equal(bids, rb)
