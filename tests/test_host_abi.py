@@ -39,6 +39,21 @@ def test_registry_names():
     assert [e.name for e in registry()] == ["laplace", "poisson", "screened_poisson", "helmholtz"]
 
 
+def test_registry_entry_rejects_several_ranks(tmp_path):
+    """The entries run one process per solve: a multi-rank call fails with 1,
+    the reference's failure code, before touching the mesh, the output or a
+    GPU."""
+    from walk_on_spheres_b200.solver import registry
+    out = tmp_path / "never.h5"
+    for e in registry():
+        for run in (e.run_2D, e.run_3D):
+            assert run(1, 2, b"missing.obj", str(out).encode(), 4, 4, 1, 10, 1e-2, 1000, 12, 1,
+                       5.0, 0) == 1
+            assert run(0, 2, b"missing.obj", str(out).encode(), 4, 4, 1, 10, 1e-2, 1000, 12, 1,
+                       5.0, 0) == 1
+    assert not out.exists()
+
+
 def read_obj(path):
     L = _lib.lib()
     f = L.wos_read_obj
