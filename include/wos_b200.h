@@ -436,11 +436,16 @@ int wos_closest_points(wos_context *ctx, int precision, const double *points, lo
                        double *dist, double *nearest, int *boundary_id);
 
 /* Lower bounds of the boundary distance that FAST_FP32 walks take from the
- * mesh's distance lattice (no reference counterpart): FP64 distances at the
- * nodes of a regular lattice over the bounding box, minus the distance to
- * the nearest node, so bound <= the exact distance everywhere.  A walk step
- * whose bound (times 1 - 2^-10) stays outside the epsilon shell uses it as
- * its radius instead of a closest-point query; WoS is unbiased for any ball
+ * mesh's distance lattice (no reference counterpart).  The lattice is a
+ * regular grid of nodes over the bounding box, 2048 along the longest axis
+ * in 2D, 256 in 3D.  Each node stores a lower bound of its boundary
+ * distance D, in FP32: the pruned FP32 query's distance times 1 - 2^-10,
+ * minus an FP32 rounding margin.  The bound at a point is that node value
+ * of its nearest node minus r, the distance to that node, so
+ * bound <= the exact distance everywhere.
+ * A walk step takes the bound times 1 - 2^-10 as its radius, instead of a
+ * closest-point query, when three conditions hold: D >= 2 r, that radius is
+ * positive, and it stays outside the epsilon shell.  WoS is unbiased for any ball
  * inside the domain.  NaN when the mesh has no lattice (meshes of at most 64
  * segments or 32 triangles, or WOS_BOUND_GRID=0). */
 int wos_distance_bounds(wos_context *ctx, const double *points, long long n, double *bound);
