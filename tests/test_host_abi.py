@@ -5,6 +5,7 @@ checked on a libhdf5-written file)."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 from pathlib import Path
 
@@ -364,3 +365,28 @@ def test_obj_edge_cases_match_reference(tmp_path, reference, name):
     assert np.array_equal(prims, rp)
     if dim == 2:
         assert np.array_equal(bids, rb)
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the built CUDA library the package raises: there is no CPU
+    fallback for any solve."""
+    import subprocess
+    import sys
+    code = ("from walk_on_spheres_b200 import Solver\n"
+            "try:\n    Solver(0)\nexcept ImportError as e:\n    print('ImportError:', e)\n")
+    env = dict(os.environ, WOS_B200_LIB=str(tmp_path / "absent.so"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       cwd=ROOT, env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "ImportError:" in r.stdout and "no CPU fallback" in r.stdout
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    """On a machine without a CUDA device, creating a context fails with the
+    CUDA status instead of computing anything on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from walk_on_spheres_b200 import Solver
+    with pytest.raises(RuntimeError):
+        Solver(0)
