@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define WOS_B200_ABI_VERSION 1
+#define WOS_B200_ABI_VERSION 2
 
 /* status codes */
 enum {
@@ -103,6 +103,10 @@ typedef struct {
     float classify_ms;              /* device time of the classification kernel */
     float walk_ms;                  /* device time of the walk kernel(s) */
     float total_ms;                 /* device time of the whole solve */
+    long long exact_queries;        /* walk steps that ran a BVH closest-point query
+                                       (bvh_npq, src/bvh.cpp:295-387): every step of
+                                       PLAIN_FP64 / FAST_FP64; FAST_FP32 steps that take
+                                       their radius from the distance lattice run none */
 } wos_counters;
 
 /* ---------------------------------------------------------------- context */
@@ -165,14 +169,16 @@ int wos_solve_grid_device(wos_context *ctx, const wos_params *params, const wos_
 /* As wos_solve_grid_device, but allocating no device memory; it has no
  * counterpart in the reference.  For callers that cannot call cudaMalloc
  * while they solve (an allocator or pool that owns the device budget, code
- * that must not synchronise the device, hosts that forbid allocation after
- * start-up).  Temporaries live in one static 8 MiB device array inside the
- * library, so grids are limited to 103 000 points (WOS_ERR_INVALID beyond);
- * the FAST methods run one walk task per point.  The first call on a device
- * looks up the array's device address (call it once before any stream
- * capture); calls that overlap on the GPU share the array and race, so
- * serialise them.  The context (mesh upload) is set up by the allocating
- * entry points beforehand. */
+ * that must not take the device-wide synchronisation cudaMalloc / cudaFree
+ * can cause, hosts that forbid allocation after start-up).  Temporaries live
+ * in one static 8 MiB device array inside the library, reserved on a device
+ * when a context is created there (wos_context_create takes its address) and
+ * held until the process exits, so grids are limited to about 94 000 points
+ * (WOS_ERR_INVALID beyond).  Arguments are checked by the same rules as
+ * wos_solve_grid_device.  The call still blocks until the solve has finished
+ * on the context's stream.  Calls that overlap on the GPU share the array and
+ * race, so serialise them.  The context (mesh upload) is set up by the
+ * allocating entry points beforehand. */
 int wos_solve_grid_device_noalloc(wos_context *ctx, const wos_params *params,
                                   const wos_grid *grid, double *mean, double *variance,
                                   double *standard_error, double *mean_steps, uint8_t *location,

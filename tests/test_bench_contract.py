@@ -41,3 +41,59 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_reference_arm_times_each_step_and_reports_the_gpu_arms_config():
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps",
+                        "2", "--warmup", "1"], capture_output=True, text=True, cwd=ROOT,
+                       timeout=300, env={k: v for k, v in os.environ.items()
+                                         if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")})
+    assert r.returncode == 0, r.stderr
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][0])
+    sys.path.insert(0, str(ROOT))
+    import bench
+    # the measured wall time of a step, not a budget
+    assert 0.0 < d["ms_per_step"] < 120000.0
+    # the same workload keys as the GPU arm's line
+    assert d["config"] == bench.CONFIG
+    assert "2 timed steps" in d["cpu_baseline"]["sample"]
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, str(ROOT))
+    import bench
+    secs, counts = bench.reduce_over_ranks(dist, "cpu", 1.0 + rank, [10.0 * (rank + 1), 1.0])
+    q.put((rank, secs, counts))
+    dist.destroy_process_group()
+
+
+def test_bench_reduces_time_by_max_and_counts_by_sum_over_two_gloo_ranks():
+    import multiprocessing as mp
+    sys.path.insert(0, str(ROOT))
+    import bench
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = bench.free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, secs, counts in got:
+        assert secs == 2.0            # the slowest rank's time
+        assert counts == [30.0, 2.0]  # walks and the like summed over ranks
+
+
+def test_bench_gpus_flag_relaunches_one_process_per_gpu():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    cmd = bench.launch_command(["--gpus", "4", "--steps", "3"], 4, 29512)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "--master-addr=127.0.0.1" in cmd
+    assert cmd[-4:] == ["--gpus", "4", "--steps", "3"]
+    assert bench.parse(["--gpus", "2", "--scaling", "strong"]).scaling == "strong"

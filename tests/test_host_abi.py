@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.wos_abi_version() == 1
+    assert L.wos_abi_version() == 2
     assert set(_lib.SIGNATURES) <= set(names)
 
 

@@ -45,7 +45,8 @@ class Counters(C.Structure):
                 ("total_walks", C.c_longlong), ("total_steps", C.c_longlong),
                 ("sum_variance", C.c_double), ("sum_standard_error", C.c_double),
                 ("sum_mean_steps", C.c_double), ("effective_epsilon", C.c_double),
-                ("classify_ms", C.c_float), ("walk_ms", C.c_float), ("total_ms", C.c_float)]
+                ("classify_ms", C.c_float), ("walk_ms", C.c_float), ("total_ms", C.c_float),
+                ("exact_queries", C.c_longlong)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

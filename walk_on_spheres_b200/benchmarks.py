@@ -5,6 +5,7 @@
     python -m walk_on_spheres_b200.benchmarks --heat [--scale 1.0]
     python -m walk_on_spheres_b200.benchmarks --transient [--scale 1.0]
     python -m walk_on_spheres_b200.benchmarks --stationary [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks --profile sphere [--walks 512]
 
 Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 
@@ -113,7 +114,8 @@ def run(name: str, scale: float = 1.0, device: int = 0, tune: bool = False) -> d
         out["methods"][method] = {
             "walks": n,
             "walks_per_s": c["total_walks"] / secs,
-            "queries_per_s": c["total_steps"] / secs,
+            "queries_per_s": c["exact_queries"] / secs,
+            "lattice_step_share": 1.0 - c["exact_queries"] / max(1, c["total_steps"]),
             "walk_ms": c["walk_ms"], "classify_ms": c["classify_ms"],
             "mean_steps": float(np.mean(r.mean_steps[ins])),
             "variance_per_walk": float(np.mean(r.variance[ins])),
@@ -221,7 +223,7 @@ def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
            "prims": [int(m.prims.shape[0]) for m in built],
            "host_build_and_upload_s": host_build_s,
            "batch_graph_ms": ms, "batch_walks_per_s": info["walks"] / (ms / 1000.0),
-           "batch_queries_per_s": info["steps"] / (ms / 1000.0)}
+           "batch_walk_steps_per_s": info["steps"] / (ms / 1000.0)}
     ms_stream = b.run(use_graph=False)
     out["batch_stream_ms"] = ms_stream
     b.close()
@@ -271,7 +273,7 @@ def run_heat(scale: float = 1.0, device: int = 0, seed: int = 7) -> dict:
             "forward_ms": c["total_ms"], "backward_ms": ca["total_ms"],
             "gradients_per_s": 1000.0 / ca["total_ms"],
             "walks_per_s": c["total_walks"] / (c["walk_ms"] / 1000.0),
-            "queries_per_s": c["total_steps"] / (c["walk_ms"] / 1000.0),
+            "queries_per_s": c["exact_queries"] / (c["walk_ms"] / 1000.0),
             "mean_steps": c["total_steps"] / max(1, c["total_walks"]),
             "probes_felt": int(felt.sum()),
             "median_rel_se_u": float(np.median(rel)),
@@ -336,6 +338,42 @@ def run_stationary(scale: float = 1.0, device: int = 0) -> dict:
     return out
 
 
+PROFILE_CASES = ("annulus", "disk_uniform", "disk_green", "sphere", "heat")
+
+
+def run_profile(case: str, walks: int, device: int = 0) -> dict:
+    """One small warm-up solve, then ONE FAST_FP32 solve of a workload at
+    `walks` walks per point: the launch an ncu capture selects with
+    `-k regex:<kernel> -s 1 -c 1` (the lattice build and the warm-up solve's
+    launches come first).  Prints the launch's walk counters, so its
+    per-step figures can be formed."""
+    s = Solver(device)
+    if case == "heat":
+        from .heat import HeatProblem
+        s.set_mesh(meshes.slab_box(target_triangles=20000))
+        rng = np.random.default_rng(20240)
+        probes = np.array([0.10, 0.05, 0.01]) * rng.uniform(0.001, 0.999, size=(4096, 3))
+        theta = (1e3, (0.05, 0.025, 0.01), 2e-3)
+        heat = HeatProblem(s, probes[:64], N_walks=16, epsilon=1e-5, seed=12345,
+                           source_mode="green", method="fast")
+        heat.adjoint(*theta)
+        heat = HeatProblem(s, probes, N_walks=walks, epsilon=1e-5, seed=12345,
+                           source_mode="green", method="fast")
+        c = heat.adjoint(*theta).counters
+    else:
+        name = {"annulus": "laplace2d_annulus256_64sq",
+                "disk_uniform": "poisson2d_circle1024_256sq_uniform",
+                "disk_green": "poisson2d_circle1024_256sq_green",
+                "sphere": "screened3d_sphere16128_64cube"}[case]
+        w = WORKLOADS[name]
+        s.set_mesh(w["mesh"]())
+        s.solve_grid(w["eq"], 8, 8, 8, N_walks=16, method="fast", **w["kw"])
+        c = s.solve_grid(w["eq"], *w["grid"], N_walks=walks, method="fast", **w["kw"]).counters
+    s.close()
+    keys = ("total_walks", "total_steps", "exact_queries", "walk_ms", "total_ms")
+    return {"case": case, "walks": walks, **{k: c[k] for k in keys}}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -352,7 +390,13 @@ def main(argv=None) -> int:
                     help="run the transient plate heating workload (reference level 2)")
     ap.add_argument("--stationary", action="store_true",
                     help="run the stationary plate heating workload (reference level 1)")
+    ap.add_argument("--profile", choices=PROFILE_CASES,
+                    help="one FAST_FP32 solve of a workload for an ncu capture (walks: --walks)")
+    ap.add_argument("--walks", type=int, default=512, help="walks per point of --profile")
     a = ap.parse_args(argv)
+    if a.profile:
+        print(json.dumps(run_profile(a.profile, a.walks, a.device)), flush=True)
+        return 0
     if a.stationary:
         print(json.dumps(run_stationary(a.scale, a.device)), flush=True)
         return 0

@@ -205,10 +205,8 @@ int wos_batch::plan() {
         b.point_begin = points;
         b.task_off = tasks;
         FastPlan pl{};
-        pl.chunk = chunk_override > 0 ? std::min(chunk_override, b.p.N_walks)
-                                      : std::min(b.p.N_walks, 1024);
-        pl.chunks = (b.p.N_walks + pl.chunk - 1) / pl.chunk;
-        pl.n_tasks = b.n * pl.chunks;
+        set_chunk(pl, chunk_override > 0 ? chunk_override : 1024, b.p.N_walks, b.p.max_steps,
+                  b.n);
         plans[order[i]] = pl;
         points += b.n;
         tasks += pl.n_tasks;
@@ -543,6 +541,7 @@ extern "C" int wos_batch_result(wos_batch *batch, int solve_id, double *mean, do
         c.indeterminate_points = static_cast<long long>(hc.indeterminate_points);
         c.total_walks = static_cast<long long>(hc.total_walks);
         c.total_steps = static_cast<long long>(hc.total_steps);
+        c.exact_queries = static_cast<long long>(hc.exact_queries);
         c.effective_epsilon = effective_epsilon(s.p);
         long long inside = 0;
         for (long long t = 0; t < s.n; ++t) {

@@ -124,6 +124,13 @@ extern "C" int wos_context_create(int device, wos_context **out) {
             return cuda_fail(nullptr, e, "cudaEventCreate");
         }
     }
+    // the allocation-free entry point's scratch array: looking its address
+    // up here loads (and so reserves) it now, while allocating is allowed
+    e = noalloc_scratch_address(&ctx->noalloc_scratch);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(nullptr, e, "cudaGetSymbolAddress (static scratch array)");
+    }
     *out = ctx;
     return WOS_OK;
 }
@@ -321,7 +328,7 @@ double wosb::effective_epsilon(const wos_params &p) {
     return p.epsilon;
 }
 
-static std::string check_params(const wos_context *ctx, const wos_params *p) {
+std::string wosb::check_params(const wos_context *ctx, const wos_params *p) {
     if (!p) return "null params";
     if (!ctx->has_mesh) return "no mesh uploaded";
     if (p->equation < 0 || p->equation > 3) return "unknown equation kind";
@@ -373,11 +380,8 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     } else {
         const int precision = p.method == WOS_METHOD_FAST_FP32 ? 32 : 64;
         FastPlan plan = plan_fast(view, wide, n, p.N_walks, precision, sms, smem_optin);
-        if (chunk_override > 0) {
-            plan.chunk = std::min(chunk_override, p.N_walks);
-            plan.chunks = (p.N_walks + plan.chunk - 1) / plan.chunk;
-            plan.n_tasks = n * plan.chunks;
-        }
+        set_chunk(plan, chunk_override > 0 ? chunk_override : plan.chunk, p.N_walks, p.max_steps,
+                  n);
         if (blocks_override > 0) plan.blocks = blocks_override;
         WOS_CUDA(this, partials.reserve(sizeof(TaskPartial) * std::max<long long>(plan.n_tasks, 1)),
                  "alloc partials");
@@ -407,6 +411,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
         c.indeterminate_points = static_cast<long long>(hc.indeterminate_points);
         c.total_walks = static_cast<long long>(hc.total_walks);
         c.total_steps = static_cast<long long>(hc.total_steps);
+        c.exact_queries = static_cast<long long>(hc.exact_queries);
         c.inside_points = p.N_walks > 0 ? c.total_walks / p.N_walks : 0;
         c.effective_epsilon = eps;
         cudaEventElapsedTime(&c.classify_ms, events[0], events[1]);
@@ -417,7 +422,7 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     return WOS_OK;
 }
 
-static PointSet grid_points(int dim, const wos_grid &g) {
+PointSet wosb::grid_points(int dim, const wos_grid &g) {
     PointSet ps{};
     ps.dim = dim;
     ps.Nx = g.Nx;
@@ -433,7 +438,7 @@ static PointSet grid_points(int dim, const wos_grid &g) {
     return ps;
 }
 
-static std::string check_grid(int dim, const wos_grid *g) {
+std::string wosb::check_grid(int dim, const wos_grid *g) {
     if (!g) return "null grid";
     if (g->Nx < 1 || g->Ny < 1 || (dim == 3 && g->Nz < 1)) return "grid sizes must be >= 1";
     const double v[6] = {g->xmin, g->xmax, g->ymin, g->ymax, g->zmin, g->zmax};

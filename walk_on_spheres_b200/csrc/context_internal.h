@@ -38,6 +38,19 @@ struct SceneDevice {
 
 double effective_epsilon(const wos_params &p);
 
+// Argument checks shared by the grid entry points: an empty string when
+// `p` (against the context's mesh) or the grid is acceptable, else the
+// reason.
+std::string check_params(const wos_context *ctx, const wos_params *p);
+std::string check_grid(int dim, const wos_grid *g);
+// The points of a Cartesian grid of a `dim`-dimensional mesh.
+PointSet grid_points(int dim, const wos_grid &g);
+
+// Device address of the allocation-free entry point's static scratch array
+// on the current device (noalloc.cu).  Taking it loads the array's module,
+// which reserves the array, so the context does it once at creation.
+cudaError_t noalloc_scratch_address(void **ptr);
+
 // Frees a batch's device memory and detaches it from its context (called
 // for every live batch when the context is destroyed).
 void detach_batch(wos_batch *batch);
@@ -87,6 +100,10 @@ struct wos_context {
     // tuning overrides (<= 0: automatic)
     int chunk_override = 0;
     int blocks_override = 0;
+
+    // this device's address of the allocation-free entry point's static
+    // scratch array, taken when the context is created
+    void *noalloc_scratch = nullptr;
 
     ~wos_context();
     std::vector<wosb::DeviceBuffer *> all_buffers();

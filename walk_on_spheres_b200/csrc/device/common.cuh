@@ -74,6 +74,9 @@ struct DeviceCounters {
     unsigned long long total_walks;
     unsigned int error_flags;   // bit 0: a rejection sampler hit its cap
     unsigned int pad;
+    // closest-point queries that traversed the BVH (FAST_FP32 lattice steps
+    // take their radius without one; every PLAIN_FP64 / FAST_FP64 step is one)
+    unsigned long long exact_queries;
 };
 
 // error_flags bits: a bounded rejection loop ran out; a walk reached a state

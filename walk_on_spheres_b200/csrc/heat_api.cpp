@@ -39,11 +39,7 @@ int wos_context::run_heat(const wos_params &p, const HeatDesc &h, const PointSet
     WOS_CUDA(this, cudaEventRecord(events[1], stream), "event");
     const int precision = p.method == WOS_METHOD_FAST_FP32 ? 32 : 64;
     FastPlan plan = plan_fast(view, wide, n, p.N_walks, precision, sms, smem_optin);
-    if (chunk_override > 0) {
-        plan.chunk = std::min(chunk_override, p.N_walks);
-        plan.chunks = (p.N_walks + plan.chunk - 1) / plan.chunk;
-        plan.n_tasks = n * plan.chunks;
-    }
+    set_chunk(plan, chunk_override > 0 ? chunk_override : plan.chunk, p.N_walks, p.max_steps, n);
     if (blocks_override > 0) plan.blocks = blocks_override;
     WOS_CUDA(this, partials.reserve(sizeof(HeatPartial) * std::max<long long>(plan.n_tasks, 1)),
              "alloc partials");
@@ -69,6 +65,7 @@ int wos_context::run_heat(const wos_params &p, const HeatDesc &h, const PointSet
         c.indeterminate_points = static_cast<long long>(hc.indeterminate_points);
         c.total_walks = static_cast<long long>(hc.total_walks);
         c.total_steps = static_cast<long long>(hc.total_steps);
+        c.exact_queries = static_cast<long long>(hc.exact_queries);
         c.inside_points = p.N_walks > 0 ? c.total_walks / p.N_walks : 0;
         c.effective_epsilon = p.epsilon;
         cudaEventElapsedTime(&c.classify_ms, events[0], events[1]);

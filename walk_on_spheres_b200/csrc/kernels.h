@@ -43,6 +43,7 @@ struct TaskPartial {
     double mean;     // Welford mean
     double m2;       // Welford M2
     double steps;    // sum of steps
+    double queries;  // closest-point queries that traversed the BVH
     unsigned int hits;
     unsigned int pad;
 };
@@ -126,6 +127,23 @@ cudaError_t launch_walk_fast(const SceneView &s, const WideView &w, const PointS
 FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, int n_walks,
                    int precision, int device_sms, size_t smem_optin);
 
+// Sets the walks per task of `plan` to `chunk` (clamped to [1, n_walks]) and
+// recomputes its task counts.  A task counts its closest-point queries, at
+// most chunk * max_steps, in 32 bits, and each lane sums the steps of its
+// ceil(chunk/32) walks in 32 bits, so the chunk is also capped at
+// floor((2^32 - 1) / max_steps), which keeps both below 2^32 and 2^31.
+inline void set_chunk(FastPlan &plan, long long chunk, int n_walks, int max_steps,
+                      long long n_points) {
+    const long long per_task = 4294967295LL / (max_steps > 0 ? max_steps : 1);
+    const long long cap = per_task < (1LL << 30) ? per_task : (1LL << 30);
+    if (chunk > cap) chunk = cap;
+    if (chunk > n_walks) chunk = n_walks;
+    if (chunk < 1) chunk = 1;
+    plan.chunk = static_cast<int>(chunk);
+    plan.chunks = static_cast<int>((n_walks + chunk - 1) / chunk);
+    plan.n_tasks = n_points * plan.chunks;
+}
+
 // Gaussian heat source -Δu = Q exp(-|x - x0|^2 / sigma^2) with per-vertex
 // Dirichlet data (kernels_adjoint.cu).
 struct HeatDesc {
@@ -144,7 +162,7 @@ struct HeatDesc {
 // sums and sums of squares of the five source-parameter derivatives
 // (Q, x0.x, x0.y, x0.z, sigma) in adjoint mode.
 struct HeatPartial {
-    double n, mean, m2, steps;
+    double n, mean, m2, steps, queries;
     double jsum[5];
     double jsq[5];
     unsigned int hits;

@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             for (int k = 0; k < 10; ++k) s_acc[k][threadIdx.x] = 0.0;
         }
         unsigned hits = 0;
+        unsigned queries = 0;  // BVH queries of this task (FP32; warp-uniform; < 2^32)
         bool bad = false;  // a closest-point query found no primitive
 
         int walk = w0 + lane;
@@ -363,6 +364,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             }
             if constexpr (kF32) {
                 unsigned pending = __ballot_sync(kFull, need_query);
+                queries += __popc(pending);
                 float qbest = 0.0f;
                 int qslot = -1;
                 while (pending) {
@@ -453,6 +455,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             hp.mean = mean_acc;
             hp.m2 = m2_acc;
             hp.steps = static_cast<double>(steps_tot);
+            hp.queries = kF32 ? static_cast<double>(queries) : static_cast<double>(steps_tot);
             hp.hits = hits;
             hp.pad = 0;
 #pragma unroll
@@ -479,13 +482,14 @@ __global__ void heat_merge_kernel(HeatArgs a, HeatOut out) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) jm[k] = js[k] = dnan();
         if (where == 1) {
-            double n = 0.0, m = 0.0, m2 = 0.0, steps = 0.0, sum[5] = {0, 0, 0, 0, 0},
-                   sq[5] = {0, 0, 0, 0, 0};
+            double n = 0.0, m = 0.0, m2 = 0.0, steps = 0.0, queries = 0.0,
+                   sum[5] = {0, 0, 0, 0, 0}, sq[5] = {0, 0, 0, 0, 0};
             unsigned long long hits = 0;
             for (int c = 0; c < a.chunks; ++c) {
                 const HeatPartial &hp = a.partials[p * a.chunks + c];
                 chan_merge(n, m, m2, hp.n, hp.mean, hp.m2);
                 steps += hp.steps;
+                queries += hp.queries;
                 hits += hp.hits;
                 if (adj) {
 #pragma unroll
@@ -516,6 +520,7 @@ __global__ void heat_merge_kernel(HeatArgs a, HeatOut out) {
             }
             if (hits) atomicAdd(&a.ctr->max_steps_hits, hits);
             atomicAdd(&a.ctr->total_steps, static_cast<unsigned long long>(steps));
+            atomicAdd(&a.ctr->exact_queries, static_cast<unsigned long long>(queries));
             atomicAdd(&a.ctr->total_walks, static_cast<unsigned long long>(n));
         } else if (where == 2) {
             const StartRecord st = a.start[p];

@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(kExactThreads)
         if (out.mean_steps) out.mean_steps[t] = mean_steps;
         if (hits) atomicAdd(&ctr->max_steps_hits, static_cast<unsigned long long>(hits));
         atomicAdd(&ctr->total_steps, steps_sum);
+        atomicAdd(&ctr->exact_queries, steps_sum);  // one FP64 BVH query per step
         atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n_walks));
         if (overflow) atomicOr(&ctr->error_flags, kErrRejectionCap);
     }

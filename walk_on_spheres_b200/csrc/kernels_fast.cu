@@ -54,6 +54,9 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     int n_acc = 0, steps_acc = 0;
     double mean_acc = 0.0, m2_acc = 0.0;
     unsigned hits = 0;
+    // BVH closest-point queries of this task (warp-uniform; FP32 only: every
+    // FP64 step is one).  At most chunk * max_steps < 2^32 (set_chunk).
+    unsigned queries = 0;
     bool overflow = false;
     bool bad = false;  // a closest-point query found no primitive
 
@@ -160,6 +163,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         }
         if constexpr (kF32 && HC == kLaneScan) {
             // a handful of primitives: every lane scans them for its own query
+            queries += __popc(__ballot_sync(kFull, need_query));
             if (need_query) {
                 const WideResult q = lane_nearest<DIM>(wv, static_cast<float>(p.x),
                                                        static_cast<float>(p.y),
@@ -171,6 +175,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         } else if constexpr (kF32) {
             // the warp resolves every pending closest-point query together
             unsigned pending = __ballot_sync(kFull, need_query);
+            queries += __popc(pending);
             float qbest = 0.0f;
             int qslot = -1;
             while (pending) {
@@ -240,6 +245,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         tp.mean = mean_acc;
         tp.m2 = m2_acc;
         tp.steps = static_cast<double>(steps_tot);
+        tp.queries = kF32 ? static_cast<double>(queries) : static_cast<double>(steps_tot);
         tp.hits = hits;
         tp.pad = 0;
         a.partials[task] = tp;
@@ -343,12 +349,13 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS)
 __device__ __forceinline__ void merge_point(long long p, int chunks, int n_walks,
                                             const TaskPartial *__restrict__ partials,
                                             const Fields &out, DeviceCounters *ctr) {
-    double n = 0.0, mean = 0.0, m2 = 0.0, steps = 0.0;
+    double n = 0.0, mean = 0.0, m2 = 0.0, steps = 0.0, queries = 0.0;
     unsigned long long hits = 0;
     for (int c = 0; c < chunks; ++c) {
         const TaskPartial tp = partials[p * chunks + c];
         chan_merge(n, mean, m2, tp.n, tp.mean, tp.m2);
         steps += tp.steps;
+        queries += tp.queries;
         hits += tp.hits;
     }
     const double variance = n_walks > 1 ? m2 / static_cast<double>(n_walks - 1) : 0.0;
@@ -358,6 +365,7 @@ __device__ __forceinline__ void merge_point(long long p, int chunks, int n_walks
     if (out.mean_steps) out.mean_steps[p] = steps / static_cast<double>(n_walks);
     if (hits) atomicAdd(&ctr->max_steps_hits, hits);
     atomicAdd(&ctr->total_steps, static_cast<unsigned long long>(steps));
+    atomicAdd(&ctr->exact_queries, static_cast<unsigned long long>(queries));
     atomicAdd(&ctr->total_walks, static_cast<unsigned long long>(n));
 }
 

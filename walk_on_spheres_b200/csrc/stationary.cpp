@@ -211,11 +211,8 @@ extern "C" int wos_stationary_solve(wos_context *ctx, const wos_stationary_param
         const int precision = p.method == WOS_METHOD_FAST_FP64 ? 64 : 32;
         FastPlan plan =
             plan_fast(dev.view, dev.wide, n, p.walks, precision, ctx->sms, ctx->smem_optin);
-        if (ctx->chunk_override > 0) {
-            plan.chunk = std::min(ctx->chunk_override, p.walks);
-            plan.chunks = (p.walks + plan.chunk - 1) / plan.chunk;
-            plan.n_tasks = n * plan.chunks;
-        }
+        set_chunk(plan, ctx->chunk_override > 0 ? ctx->chunk_override : plan.chunk, p.walks,
+                  p.max_steps, n);
         if (ctx->blocks_override > 0) plan.blocks = ctx->blocks_override;
         WOS_CUDA(ctx, d_part.reserve(sizeof(TaskPartial) * plan.n_tasks), "alloc partials");
         WOS_CUDA(ctx, d_queue.reserve(sizeof(unsigned long long)), "alloc queue");

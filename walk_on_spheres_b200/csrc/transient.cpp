@@ -286,9 +286,7 @@ extern "C" int wos_transient_solve(wos_context *ctx, const wos_transient_params 
         long long chunk = static_cast<long long>(p.walks) * n / (2 * resident);
         chunk = std::max<long long>(256, std::min<long long>(1024, chunk));
         if (ctx->chunk_override > 0) chunk = ctx->chunk_override;
-        plan.chunk = static_cast<int>(std::min<long long>(chunk, p.walks));
-        plan.chunks = (p.walks + plan.chunk - 1) / plan.chunk;
-        plan.n_tasks = n * plan.chunks;
+        set_chunk(plan, chunk, p.walks, p.max_steps, n);
         if (ctx->blocks_override > 0) plan.blocks = ctx->blocks_override;
         WOS_CUDA(ctx, d_part.reserve(sizeof(TaskPartial) * plan.n_tasks), "alloc partials");
         WOS_CUDA(ctx, d_queue.reserve(sizeof(unsigned long long)), "alloc queue");
