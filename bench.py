@@ -88,12 +88,12 @@ METHOD_NAMES = {"fast": "FAST_FP32 (FP32 walk + FP64 epsilon shell, FP64 sums)",
 # The reference arm's slices: step s solves the grid points whose linear
 # index is congruent to s modulo REF_STRIDE.
 REF_STRIDE = 128
-# Per walk step of walk_fast_kernel on this workload (FAST_FP32, 4096 walks),
-# from one ncu capture of each source mode's launch (the capture commands and
-# figures: profiles/walk_fast_kernel_poisson2d_circle1024.md): warp
-# instructions issued (sm__inst_issued.sum), L2 bytes (lts__t_bytes.sum) and
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum), each divided by
-# the launch's walk steps, and the L2 peak ncu reports for the part.
+# Per walk step of walk_fast_kernel on this workload (FAST_FP32), from one
+# ncu capture of each source mode's launch (`python -m
+# walk_on_spheres_b200.benchmarks --profile disk_uniform` / `disk_green`):
+# warp instructions issued (sm__inst_issued.sum), L2 bytes (lts__t_bytes.sum)
+# and DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum), each divided
+# by the launch's walk steps, and the L2 peak ncu reports for the part.
 NCU_PER_STEP = {"uniform": {"issued": None, "l2_bytes": None, "dram_bytes": None},
                 "green": {"issued": None, "l2_bytes": None, "dram_bytes": None}}
 NCU_L2_PEAK_GBS = None

@@ -489,8 +489,48 @@ typedef struct {
 } wos_equation_entry;
 
 /* The registry: laplace, poisson, screened_poisson, helmholtz
- * (src/equations/equations.hpp:26-31). */
+ * (src/equations/equations.hpp:26-31).  With size == 1 an entry sweeps the
+ * whole grid on the GPU named by WOS_B200_DEVICE (default 0).  With size > 1
+ * (the reference's `mpirun -np P wos ...`, README.md:32) rank `rank` solves
+ * the reference's Cartesian block of the grid (include/wos/runner.hpp:90-134,
+ * rank blocks from MPI_Dims_create) on GPU rank % device count (or
+ * WOS_B200_DEVICE), the counters are reduced over the ranks
+ * (runner.hpp:240-263), rank 0 creates the result file and every rank writes
+ * its block into it (include/wos/hdf5_io.hpp:51-171).  The ranks meet only
+ * through the collectives installed with wos_set_collectives; without them a
+ * call with size > 1 fails with 1. */
 const wos_equation_entry *wos_equation_registry(int *count);
+
+/* The caller's process-group collectives, used by the registry entries when
+ * size > 1 in place of the reference's MPI calls (MPI_Barrier, MPI_Reduce /
+ * MPI_Allreduce, MPI_Dims_create in include/wos/runner.hpp:90-263 and
+ * include/wos/hdf5_io.hpp:51-171).  Every callback returns 0 on success.
+ *  barrier:     return once every rank has entered it.
+ *  allreduce:   reduce `n` doubles in place over the ranks, every rank
+ *               receiving the result; op WOS_REDUCE_SUM or WOS_REDUCE_MAX.
+ *  dims_create: optional (NULL: the library's restatement of MPI_Dims_create,
+ *               a balanced factorisation in non-increasing order); fill the
+ *               zero entries of dims[3] for `size` ranks, as MPI_Dims_create
+ *               does. */
+enum { WOS_REDUCE_SUM = 0, WOS_REDUCE_MAX = 1 };
+typedef struct {
+    int (*barrier)(void *user);
+    int (*allreduce)(double *values, int n, int op, void *user);
+    int (*dims_create)(int size, int dims[3], void *user);
+    void *user;
+} wos_collectives;
+
+/* Install (or, with NULL, remove) the collectives for this process.
+ * WOS_ERR_INVALID if barrier or allreduce is missing. */
+int wos_set_collectives(const wos_collectives *collectives);
+
+/* Rank `rank`'s block of an Nx x Ny x Nz grid split over `size` ranks as the
+ * reference splits it (include/wos/runner.hpp:90-134): the decomposition
+ * dims[3], the block's first grid index offset[3] and extent count[3] along
+ * x, y, z.  WOS_ERR_INVALID with the reference's message in `error` (may be
+ * NULL) when the ranks do not fit the grid.  Host only. */
+int wos_rank_block(int dim, int Nx, int Ny, int Nz, int rank, int size, int dims[3],
+                   int offset[3], int count[3], char *error, int error_capacity);
 
 /* ------------------------------------------------ host-only (no GPU needed) */
 

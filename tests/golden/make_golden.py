@@ -1,6 +1,6 @@
 """Generate the golden fixtures from the REFERENCE's own code.
 
-    make -C oracle ref        # compiles the reference sources (needs /root/reference)
+    make -C oracle ref        # compiles the reference sources ($WOS_REFERENCE_DIR)
     python tests/golden/make_golden.py
 
 Every array here is computed by oracle/_ref/libwos_ref.so, i.e. the

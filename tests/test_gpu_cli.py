@@ -83,3 +83,18 @@ def test_cli_file_matches_reference_registry(tmp_path, reference, name):
     if mesh.dim == 3:
         retries = int(ref["/metadata/ambiguous_ray_retries"].view(np.int64)[0])
         assert "ambiguous ray retries:         %d" % retries in lines
+
+
+def test_cli_file_opens_with_libhdf5(tmp_path):
+    """Where h5py (libhdf5) is installed, a `wos` result file opens with it and
+    holds the datasets the library's own reader sees."""
+    h5py = pytest.importorskip("h5py")
+    obj = meshes.write_obj(meshes.annulus(segments=32), tmp_path / "mesh.obj")
+    out = tmp_path / "ours.h5"
+    r = subprocess.run([str(WOS), "--walks", "50", "-o", str(out), "laplace", "8", "8",
+                        str(obj)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    ours = h5lite.read(out)
+    with h5py.File(out, "r") as f:
+        for key, value in ours.items():
+            assert np.array_equal(np.asarray(f[key][()]), value, equal_nan=True), key

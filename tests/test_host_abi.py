@@ -40,10 +40,10 @@ def test_registry_names():
     assert [e.name for e in registry()] == ["laplace", "poisson", "screened_poisson", "helmholtz"]
 
 
-def test_registry_entry_rejects_several_ranks(tmp_path):
-    """The entries run one process per solve: a multi-rank call fails with 1,
-    the reference's failure code, before touching the mesh, the output or a
-    GPU."""
+def test_registry_entry_rejects_several_ranks_without_collectives(tmp_path):
+    """With no collectives installed (wos_set_collectives) a multi-rank call
+    fails with 1, the reference's failure code, before touching the mesh, the
+    output or a GPU."""
     from walk_on_spheres_b200.solver import registry
     out = tmp_path / "never.h5"
     for e in registry():

@@ -98,6 +98,18 @@ RUN_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int,
                      C.c_int)
 
 
+BARRIER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_void_p)
+DIMS_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p)
+
+
+class Collectives(C.Structure):
+    """wos_collectives: the caller's barrier / all-reduce (/ dims_create) for
+    registry runs with size > 1."""
+    _fields_ = [("barrier", BARRIER_FN), ("allreduce", ALLREDUCE_FN),
+                ("dims_create", DIMS_FN), ("user", C.c_void_p)]
+
+
 class EquationEntry(C.Structure):
     """wos_equation_entry (src/equations/equations.hpp:7-17)."""
     _fields_ = [("name", C.c_char_p), ("run_2D", RUN_FN), ("run_3D", RUN_FN)]
@@ -152,6 +164,9 @@ SIGNATURES = {
     "wos_build_wide_bvh": (C.c_int, [C.c_int, VP, C.c_int, VP, C.c_int] + [VP] * 5),
     "wos_equation_registry": (C.POINTER(EquationEntry), [C.POINTER(C.c_int)]),
     "wos_peek_mesh_dim": (C.c_int, [C.c_char_p]),
+    "wos_set_collectives": (C.c_int, [C.POINTER(Collectives)]),
+    "wos_rank_block": (C.c_int, [C.c_int] * 6 + [C.POINTER(C.c_int)] * 3 + [C.c_char_p,
+                                                                         C.c_int]),
     # result files: serial writer and the parallel path (create, then blocks)
     "wos_write_hdf5": (C.c_int, [C.c_char_p, C.POINTER(Grid)] + [VP] * 5 + [
         C.c_int, C.c_double, C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_longlong,

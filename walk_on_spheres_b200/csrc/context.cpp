@@ -245,7 +245,20 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
         return e;
     }
     auto *out = static_cast<float *>(lattice.ptr);
-    if ((e = launch_lattice32(wide, margin, out, sms, stream)) != cudaSuccess) return e;
+    // outside-node skip: its row crossings and node mask live in a
+    // stream-ordered temporary (WOS_LATTICE_SKIP=0 queries every node)
+    void *skip = nullptr;
+    const char *skip_env = std::getenv("WOS_LATTICE_SKIP");
+    if (!(skip_env && std::string(skip_env) == "0")) {
+        if ((e = cudaMallocAsync(&skip, lattice_skip_bytes(wide), stream)) != cudaSuccess) return e;
+    }
+    const double tol = 1e-5 * std::max(mag, ext);
+    e = launch_lattice32(view, wide, margin, out, sms, skip, tol, stream);
+    if (skip) {
+        const cudaError_t f = cudaFreeAsync(skip, stream);
+        if (e == cudaSuccess) e = f;
+    }
+    if (e != cudaSuccess) return e;
     wide.gd = out;
     wide.gratio = 2.0f;  // bound >= 1/3 of the upper bound
     if (const char *env = std::getenv("WOS_LATTICE_RATIO")) {

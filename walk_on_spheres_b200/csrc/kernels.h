@@ -187,9 +187,14 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
 // unused): out[(i*gn[1] + j)*gn[2] + k] = the exact FP32 cooperative query's
 // boundary distance at the FP32 node glo + (i, j, k) * gh, minus `margin`,
 // rounded down (0 if negative).  FP64 per-thread queries took 240 ms for a
-// 173k-triangle mesh at 160^3 nodes.
-cudaError_t launch_lattice32(const WideView &w, float margin, float *out, int sms,
-                            cudaStream_t stream);
+// 173k-triangle mesh at 160^3 nodes.  With `scratch` (lattice_skip_bytes(w)
+// bytes of device memory, else null) the nodes whose own and neighbours'
+// centres lie outside the mesh, by the crossing parity of their lattice row
+// (rows within `tol` of an edge or vertex stay unclassified), store 0 without
+// a query.
+size_t lattice_skip_bytes(const WideView &w);
+cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin, float *out,
+                             int sms, void *scratch, double tol, cudaStream_t stream);
 // lattice_bound at each point (FP32), NaN where the scene has no lattice.
 cudaError_t launch_lattice_bounds(const WideView &w, const double *pts, long long n, double *out,
                                   cudaStream_t stream);

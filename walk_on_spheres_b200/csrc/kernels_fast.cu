@@ -626,17 +626,38 @@ namespace {
 // stored is sqrt(best) (1 - tau) minus `margin` (the FP32 rounding of the
 // primitive distances, a few ulps of the coordinates), rounded down.
 template <int DIM, int HC>
-__global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin, float *out) {
+__global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin,
+                                                        const uint8_t *__restrict__ outside,
+                                                        float *out) {
     constexpr float kShrink = 1.0f - 0x1p-10f;
     const int lane = threadIdx.x & 31;
     const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    constexpr int kNeighbours = DIM == 2 ? 9 : 27;
     for (long long t = warp; t < n; t += warps) {
         const int k = static_cast<int>(t % w.gn[2]);
         const long long r = t / w.gn[2];
         const int j = static_cast<int>(r % w.gn[1]);
         const int i = static_cast<int>(r / w.gn[1]);
+        if (outside != nullptr) {
+            // a node whose own and neighbours' centres are all outside the
+            // mesh stores 0 (a valid lower bound) without a query: no walk
+            // inside the domain samples it for a useful bound
+            bool out_n = true;
+            if (lane < kNeighbours) {
+                const int ni = i + lane % 3 - 1, nj = j + (lane / 3) % 3 - 1;
+                const int nk = DIM == 3 ? k + lane / 9 - 1 : 0;
+                if (ni >= 0 && ni < w.gn[0] && nj >= 0 && nj < w.gn[1] && nk >= 0 &&
+                    nk < w.gn[2]) {
+                    out_n = outside[(static_cast<long long>(ni) * w.gn[1] + nj) * w.gn[2] + nk] != 0;
+                }
+            }
+            if (__all_sync(kFull, out_n)) {
+                if (lane == 0) out[t] = 0.0f;
+                continue;
+            }
+        }
         const float x = w.glo[0] + static_cast<float>(i) * w.gh;
         const float y = w.glo[1] + static_cast<float>(j) * w.gh;
         const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
@@ -645,6 +666,136 @@ __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin
             const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
             out[t] = d > 0.0f ? d : 0.0f;
         }
+    }
+}
+
+// Outside-node classification of the lattice, by the parity of boundary
+// crossings along each lattice row (a line along x through the node centres
+// (y_j, z_k)).  kRowCrossings crossings are kept per row; a row with more, an
+// odd count, or one passing within `tol` of a primitive's edge or vertex is
+// left unclassified (none of its nodes is skipped).  Storing 0 at a node is
+// always a valid lower bound, so a wrong verdict costs walk speed, never
+// correctness.
+constexpr int kRowCrossings = 16;
+constexpr unsigned kRowUnknown = 0x80000000u;
+
+__device__ __forceinline__ void add_crossing(unsigned *count, float *cross, long long row,
+                                             float x) {
+    const unsigned c = atomicAdd(count + row, 1u) & ~kRowUnknown;
+    if (c < static_cast<unsigned>(kRowCrossings)) cross[row * kRowCrossings + c] = x;
+}
+
+// 2D: one thread per segment, rows y_j = glo[1] + j h.
+__global__ void row_crossings2_kernel(SceneView s, WideView w, double tol, unsigned *count,
+                                      float *cross) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n_prims) return;
+    const double2 a = s.seg64[2 * p], b = s.seg64[2 * p + 1];
+    const double ylo = fmin(a.y, b.y), yhi = fmax(a.y, b.y);
+    const double h = w.gh, y0 = w.glo[1];
+    const int j0 = max(0, static_cast<int>(floor((ylo - tol - y0) / h)));
+    const int j1 = min(w.gn[1] - 1, static_cast<int>(ceil((yhi + tol - y0) / h)));
+    for (int j = j0; j <= j1; ++j) {
+        const double y = static_cast<double>(w.glo[1] + static_cast<float>(j) * w.gh);
+        if (y < ylo - tol || y > yhi + tol) continue;
+        if (fabs(y - a.y) <= tol || fabs(y - b.y) <= tol) {
+            atomicOr(count + j, kRowUnknown);
+            continue;
+        }
+        const double x = a.x + (y - a.y) * (b.x - a.x) / (b.y - a.y);
+        add_crossing(count, cross, j, static_cast<float>(x));
+    }
+}
+
+// 3D: one thread per triangle, rows through (y_j, z_k); a row crosses the
+// triangle where its (y, z) projection contains (y_j, z_k).
+__global__ void row_crossings3_kernel(SceneView s, WideView w, double tol, unsigned *count,
+                                      float *cross) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n_prims) return;
+    const double2 *r = s.tri64 + 7 * p;
+    const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+    // v0 = (r0.x, r0.y, r1.x), e1 = (r1.y, r2.x, r2.y), e2 = (r3.x, r3.y, r4.x)
+    const double v0[3] = {r0.x, r0.y, r1.x};
+    const double e1[3] = {r1.y, r2.x, r2.y}, e2[3] = {r3.x, r3.y, r4.x};
+    const double P[3][2] = {{v0[1], v0[2]}, {v0[1] + e1[1], v0[2] + e1[2]},
+                            {v0[1] + e2[1], v0[2] + e2[2]}};
+    const double nx = e1[1] * e2[2] - e1[2] * e2[1];
+    const double ny = e1[2] * e2[0] - e1[0] * e2[2];
+    const double nz = e1[0] * e2[1] - e1[1] * e2[0];
+    const double ylo = fmin(fmin(P[0][0], P[1][0]), P[2][0]);
+    const double yhi = fmax(fmax(P[0][0], P[1][0]), P[2][0]);
+    const double zlo = fmin(fmin(P[0][1], P[1][1]), P[2][1]);
+    const double zhi = fmax(fmax(P[0][1], P[1][1]), P[2][1]);
+    const double h = w.gh;
+    const int j0 = max(0, static_cast<int>(floor((ylo - tol - w.glo[1]) / h)));
+    const int j1 = min(w.gn[1] - 1, static_cast<int>(ceil((yhi + tol - w.glo[1]) / h)));
+    const int k0 = max(0, static_cast<int>(floor((zlo - tol - w.glo[2]) / h)));
+    const int k1 = min(w.gn[2] - 1, static_cast<int>(ceil((zhi + tol - w.glo[2]) / h)));
+    double len[3];
+    for (int q = 0; q < 3; ++q) {
+        const double dy = P[(q + 1) % 3][0] - P[q][0], dz = P[(q + 1) % 3][1] - P[q][1];
+        len[q] = sqrt(dy * dy + dz * dz);
+    }
+    for (int j = j0; j <= j1; ++j) {
+        const double y = static_cast<double>(w.glo[1] + static_cast<float>(j) * w.gh);
+        for (int k = k0; k <= k1; ++k) {
+            const double z = static_cast<double>(w.glo[2] + static_cast<float>(k) * w.gh);
+            const long long row = static_cast<long long>(j) * w.gn[2] + k;
+            int pos = 0, neg = 0;
+            bool near = false;
+            for (int q = 0; q < 3; ++q) {
+                const double *A = P[q], *B = P[(q + 1) % 3];
+                const double c = (B[0] - A[0]) * (z - A[1]) - (B[1] - A[1]) * (y - A[0]);
+                if (fabs(c) <= tol * len[q]) near = true;
+                else if (c > 0.0) ++pos;
+                else ++neg;
+            }
+            if (near) {
+                // on or next to an edge line of the projection: undecided,
+                // unless the point is plainly outside the projected triangle
+                if (pos < 1 || neg < 1) atomicOr(count + row, kRowUnknown);
+                continue;
+            }
+            if (pos != 3 && neg != 3) continue;
+            const double x = v0[0] - (ny * (y - v0[1]) + nz * (z - v0[2])) / nx;
+            add_crossing(count, cross, row, static_cast<float>(x));
+        }
+    }
+}
+
+// One thread per row: sort its crossings and mark the nodes with an even
+// number of crossings below them (and none within tol) as outside.
+__global__ void row_outside_kernel(WideView w, double tol, const unsigned *count,
+                                   const float *cross, uint8_t *outside) {
+    const long long rows = static_cast<long long>(w.gn[1]) * w.gn[2];
+    const long long row = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (row >= rows) return;
+    const unsigned c = count[row];
+    const int m = static_cast<int>(c & ~kRowUnknown);
+    const bool known = !(c & kRowUnknown) && m <= kRowCrossings && (m % 2) == 0;
+    float xs[kRowCrossings];
+    for (int q = 0; q < kRowCrossings; ++q) xs[q] = q < m && known ? cross[row * kRowCrossings + q] : 0.0f;
+    for (int q = 1; q < m && known; ++q) {  // insertion sort
+        const float v = xs[q];
+        int u = q - 1;
+        while (u >= 0 && xs[u] > v) {
+            xs[u + 1] = xs[u];
+            --u;
+        }
+        xs[u + 1] = v;
+    }
+    int below = 0;
+    for (int i = 0; i < w.gn[0]; ++i) {
+        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+        bool out = known;
+        if (known) {
+            while (below < m && xs[below] <= x) ++below;
+            out = (below % 2) == 0;
+            if (below > 0 && static_cast<double>(x) - xs[below - 1] <= tol) out = false;
+            if (below < m && static_cast<double>(xs[below]) - x <= tol) out = false;
+        }
+        outside[static_cast<long long>(i) * rows + row] = out ? 1 : 0;
     }
 }
 
@@ -663,20 +814,48 @@ __global__ void lattice_bounds_kernel(WideView w, const double *pts, long long n
 }
 }  // namespace
 
-cudaError_t launch_lattice32(const WideView &w, float margin, float *out, int sms,
-                            cudaStream_t stream) {
+size_t lattice_skip_bytes(const WideView &w) {
+    const size_t nodes = static_cast<size_t>(w.gn[0]) * w.gn[1] * w.gn[2];
+    const size_t rows = static_cast<size_t>(w.gn[1]) * w.gn[2];
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    return up(nodes) + up(rows * sizeof(unsigned)) + up(rows * kRowCrossings * sizeof(float));
+}
+
+cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin, float *out,
+                             int sms, void *scratch, double tol, cudaStream_t stream) {
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
     if (n <= 0) return cudaSuccess;
+    uint8_t *outside = nullptr;
+    if (scratch != nullptr) {
+        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+        const size_t rows = static_cast<size_t>(w.gn[1]) * w.gn[2];
+        outside = static_cast<uint8_t *>(scratch);
+        auto *count = reinterpret_cast<unsigned *>(outside + up(static_cast<size_t>(n)));
+        auto *cross = reinterpret_cast<float *>(reinterpret_cast<char *>(count) +
+                                                up(rows * sizeof(unsigned)));
+        cudaError_t e = cudaMemsetAsync(count, 0, rows * sizeof(unsigned), stream);
+        if (e != cudaSuccess) return e;
+        const unsigned pb = static_cast<unsigned>((s.n_prims + 127) / 128);
+        if (w.dim == 2) {
+            row_crossings2_kernel<<<pb, 128, 0, stream>>>(s, w, tol, count, cross);
+        } else {
+            row_crossings3_kernel<<<pb, 128, 0, stream>>>(s, w, tol, count, cross);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        row_outside_kernel<<<static_cast<unsigned>((rows + 127) / 128), 128, 0, stream>>>(
+            w, tol, count, cross, outside);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
     // compiled per traversal class, like the walk kernels
     return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
         constexpr int HC = decltype(h)::value;
         if (w.dim == 2) {
             lattice32_kernel<2, HC>
-                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, outside, out);
         } else {
             lattice32_kernel<3, HC>
-                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, out);
+                <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, outside, out);
         }
         return cudaGetLastError();
     });

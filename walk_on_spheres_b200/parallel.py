@@ -28,7 +28,7 @@ import numpy as np
 
 FIELDS = ("mean", "variance", "standard_error", "mean_steps", "location")
 COUNTS = ("inside_points", "max_steps_hits", "ambiguous_ray_retries", "indeterminate_points",
-          "total_walks", "total_steps")
+          "total_walks", "total_steps", "exact_queries")
 
 
 def grid_size(grid, dim: int) -> int:
@@ -178,3 +178,73 @@ def solve_grid_sharded_to_file(solve_shard, grid, path, meta, group=None,
         error = e
     agree(error is None, "writing a shard")
     return total
+
+
+def rank_block(dim: int, Nx: int, Ny: int, Nz: int, rank: int, size: int):
+    """(dims, offset, count) of `rank`'s block of the grid as the reference
+    splits it over `size` MPI ranks (include/wos/runner.hpp:90-134); raises
+    ValueError with the reference's message when the ranks do not fit."""
+    import ctypes as C
+
+    from . import _lib
+    dims, off, cnt = (C.c_int * 3)(), (C.c_int * 3)(), (C.c_int * 3)()
+    err = C.create_string_buffer(256)
+    rc = _lib.lib().wos_rank_block(dim, Nx, Ny, Nz, rank, size, dims, off, cnt, err, 256)
+    if rc != 0:
+        raise ValueError(err.value.decode() or "invalid arguments")
+    return tuple(dims), tuple(off), tuple(cnt)
+
+
+class TorchCollectives:
+    """Backs the registry's multi-rank collectives (wos_set_collectives) with a
+    torch.distributed process group, in place of the reference's MPI: a
+    registry entry called with (rank, size) on every rank of the group then
+    solves its block and writes it into the shared result file.
+
+        dist.init_process_group("gloo")       # or "nccl" with device=...
+        with TorchCollectives():
+            entry.run_2D(dist.get_rank(), dist.get_world_size(), mesh, out, ...)
+
+    Reductions run on `device` (None / "cpu" for gloo)."""
+
+    def __init__(self, group=None, device=None):
+        import ctypes as C
+
+        from . import _lib
+        self.group, self.device = group, device
+        self._C = C
+        self._fns = (_lib.BARRIER_FN(self._barrier), _lib.ALLREDUCE_FN(self._allreduce),
+                     _lib.DIMS_FN())
+        self.struct = _lib.Collectives(self._fns[0], self._fns[1], self._fns[2], None)
+
+    def _barrier(self, user) -> int:
+        import torch.distributed as dist
+        try:
+            dist.barrier(group=self.group)
+            return 0
+        except Exception:
+            return 1
+
+    def _allreduce(self, values, n, op, user) -> int:
+        import torch
+        import torch.distributed as dist
+        try:
+            t = torch.tensor([values[i] for i in range(n)], dtype=torch.float64)
+            if self.device is not None and str(self.device) != "cpu":
+                t = t.to(self.device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX if op == 1 else dist.ReduceOp.SUM,
+                            group=self.group)
+            for i, v in enumerate(t.cpu().tolist()):
+                values[i] = v
+            return 0
+        except Exception:
+            return 1
+
+    def __enter__(self):
+        from . import _lib
+        _lib.check(_lib.lib().wos_set_collectives(self._C.byref(self.struct)))
+        return self
+
+    def __exit__(self, *exc):
+        from . import _lib
+        _lib.lib().wos_set_collectives(None)
