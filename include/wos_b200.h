@@ -463,6 +463,13 @@ int wos_distance_bounds(wos_context *ctx, const double *points, long long n, dou
 int wos_special_functions(wos_context *ctx, int precision, const double *x, long long n,
                           double *log_i0, double *log_k0);
 
+/* The current mesh's device scene (every tree and primitive array of
+ * wos_set_mesh, not the lattice) copied to a host buffer, for checks that the
+ * device tree build (the default; WOS_TREE_BUILD=host builds on the host
+ * threads) and the host build give the same bytes.  *bytes receives the size;
+ * out may be NULL to ask for it.  No reference counterpart. */
+int wos_scene_arena(wos_context *ctx, void *out, long long capacity, long long *bytes);
+
 /* Scheduling overrides of the FAST methods (no reference counterpart):
  * walks per task and persistent grid size; <= 0 restores the automatic
  * choice.  Used by the benchmark's tuner. */

@@ -138,6 +138,7 @@ SIGNATURES = {
     "wos_special_functions": (C.c_int, [VP, C.c_int, VP, C.c_longlong, VP, VP]),
     "wos_distance_bounds": (C.c_int, [VP, VP, C.c_longlong, VP]),
     "wos_set_tuning": (C.c_int, [VP, C.c_int, C.c_int]),
+    "wos_scene_arena": (C.c_int, [VP, VP, C.c_longlong, C.POINTER(C.c_longlong)]),
     "wos_mesh_vertex_count": (C.c_int, [VP, C.POINTER(C.c_int)]),
     "wos_transient_defaults": (None, [C.POINTER(TransientParams)]),
     "wos_transient_steps": (C.c_int, [C.POINTER(TransientParams)]),

@@ -129,6 +129,32 @@ int wos_batch::prepare() {
     std::stable_sort(todo.begin(), todo.end(), [](const BatchMesh *a, const BatchMesh *b) {
         return a->prims.size() > b->prims.size();
     });
+    if (device_tree_build()) {
+        // every tree on the device, one mesh after another on the stream,
+        // each followed by its lattice; the host only checks the meshes
+        cudaSetDevice(ctx->device);
+        for (BatchMesh *mp : todo) {
+            BatchMesh &m = *mp;
+            const std::string e =
+                scene_meta(m.dim, m.verts.data(), static_cast<int>(m.verts.size()) / m.dim,
+                           m.prims.data(), static_cast<int>(m.prims.size()) / m.dim,
+                           m.bids.empty() ? nullptr : m.bids.data(), m.leaf_size, m.scene);
+            if (!e.empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + e);
+            WOS_CUDA(ctx, m.dev.build_on_device(m.scene, ctx->stream), "batch tree build");
+            m.built = true;
+        }
+        // the mesh copies serve the build's uploads until it has run
+        WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "batch tree build");
+        for (BatchMesh *mp : todo) {
+            mp->verts.clear();
+            mp->verts.shrink_to_fit();
+            mp->prims.clear();
+            mp->prims.shrink_to_fit();
+            mp->bids.clear();
+            mp->bids.shrink_to_fit();
+        }
+        return WOS_OK;
+    }
     std::vector<std::string> errs(todo.size());
     std::vector<char> done(todo.size(), 0);
     std::mutex mu;

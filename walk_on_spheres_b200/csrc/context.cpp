@@ -149,40 +149,40 @@ extern "C" void wos_context_destroy(wos_context *ctx) {
 // One device allocation per scene (arrays at 256-byte aligned offsets): a
 // set_mesh or batch mesh costs one cudaMalloc instead of one per array.
 cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
-    struct Part {
-        const void *src;
-        size_t bytes;
-        size_t offset;
-    };
+    const ArenaLayout L = arena_layout(h);
     const std::vector<int> off(h.w_off, h.w_off + 8);
-    Part parts[] = {
-        {h.box64.data(), h.box64.size() * sizeof(double), 0},
-        {h.seg64.data(), h.seg64.size() * sizeof(double), 0},
-        {h.segid.data(), h.segid.size() * sizeof(int), 0},
-        {h.tri64.data(), h.tri64.size() * sizeof(double), 0},
-        {h.wbox.data(), h.wbox.size() * sizeof(float), 0},
-        {h.wprim.data(), h.wprim.size() * sizeof(float), 0},
-        {h.wide2bin.data(), h.wide2bin.size() * sizeof(int), 0},
-        {off.data(), off.size() * sizeof(int), 0},
-        {h.slot_verts.data(), h.slot_verts.size() * sizeof(int), 0},
-    };
-    size_t total = 0;
-    for (Part &p : parts) {
-        p.offset = total;
-        total += (std::max<size_t>(p.bytes, 16) + 255) / 256 * 256;
+    const void *src[ArenaLayout::kParts] = {h.box64.data(), h.seg64.data(), h.segid.data(),
+                                            h.tri64.data(), h.wbox.data(), h.wprim.data(),
+                                            h.wide2bin.data(), off.data(), h.slot_verts.data()};
+    const size_t have[ArenaLayout::kParts] = {
+        h.box64.size() * sizeof(double), h.seg64.size() * sizeof(double),
+        h.segid.size() * sizeof(int), h.tri64.size() * sizeof(double),
+        h.wbox.size() * sizeof(float), h.wprim.size() * sizeof(float),
+        h.wide2bin.size() * sizeof(int), off.size() * sizeof(int),
+        h.slot_verts.size() * sizeof(int)};
+    for (int k = 0; k < ArenaLayout::kParts; ++k) {
+        if (have[k] != L.bytes[k]) return cudaErrorInvalidValue;  // a builder bug
     }
-    cudaError_t e = arena.reserve(total);
+    cudaError_t e = arena.reserve(L.total);
     if (e != cudaSuccess) return e;
     auto *base = static_cast<char *>(arena.ptr);
-    if ((e = cudaMemsetAsync(base, 0, total, stream)) != cudaSuccess) return e;
-    for (const Part &p : parts) {
-        if (p.bytes == 0) continue;
-        e = cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, stream);
+    if ((e = cudaMemsetAsync(base, 0, L.total, stream)) != cudaSuccess) return e;
+    for (int k = 0; k < ArenaLayout::kParts; ++k) {
+        if (L.bytes[k] == 0) continue;
+        e = cudaMemcpyAsync(base + L.offset[k], src[k], L.bytes[k], cudaMemcpyHostToDevice,
+                            stream);
         if (e != cudaSuccess) return e;
     }
     // no wait: a copy from pageable memory returns once its source is staged,
     // and every later use of the scene is ordered after it on `stream`
-    auto at = [&](int k) { return static_cast<const void *>(base + parts[k].offset); };
+    set_views(h);
+    return build_lattice(h, stream);
+}
+
+void SceneDevice::set_views(const HostScene &h) {
+    const ArenaLayout L = arena_layout(h);
+    auto *base = static_cast<char *>(arena.ptr);
+    auto at = [&](int k) { return static_cast<const void *>(base + L.offset[k]); };
     view = SceneView{};
     view.dim = h.dim;
     view.n_prims = h.n_prims;
@@ -202,7 +202,6 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
     wide.prim = static_cast<const float *>(at(5));
     wide.wide2bin = static_cast<const int *>(at(6));
     slot_verts = static_cast<const int *>(at(8));
-    return build_lattice(h, stream);
 }
 
 // The distance lattice of the FAST_FP32 walks (device/wide.cuh): nodes
@@ -274,9 +273,18 @@ void SceneDevice::release() {
     slot_verts = nullptr;
 }
 
+bool wosb::device_tree_build() {
+    const char *e = std::getenv("WOS_TREE_BUILD");
+    return !(e && std::string(e) == "host");
+}
+
 int wos_context::upload_scene() {
     cudaSetDevice(device);
-    WOS_CUDA(this, sdev.upload(scene, stream), "mesh upload");
+    if (scene.box64.empty()) {
+        WOS_CUDA(this, sdev.build_on_device(scene, stream), "device tree build");
+    } else {
+        WOS_CUDA(this, sdev.upload(scene, stream), "mesh upload");
+    }
     view = sdev.view;
     wide = sdev.wide;
     has_mesh = true;
@@ -288,12 +296,31 @@ extern "C" int wos_set_mesh(wos_context *ctx, int dim, const double *verts, int 
                             int leaf_size) {
     if (!ctx) return fail(nullptr, WOS_ERR_INVALID, "wos_set_mesh: null context");
     HostScene sc;
+    // the device build needs only the checked mesh and its metadata
     const std::string err =
-        build_scene(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, sc);
+        device_tree_build()
+            ? scene_meta(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, sc)
+            : build_scene(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, sc);
     if (!err.empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + err);
     ctx->scene = std::move(sc);
     ctx->has_mesh = false;
     return ctx->upload_scene();
+}
+
+extern "C" int wos_scene_arena(wos_context *ctx, void *out, long long capacity,
+                               long long *bytes) {
+    if (!ctx || !ctx->has_mesh) return fail(ctx, WOS_ERR_INVALID, "wos_scene_arena: no mesh");
+    const ArenaLayout L = arena_layout(ctx->scene);
+    if (bytes) *bytes = static_cast<long long>(L.total);
+    if (!out) return WOS_OK;
+    if (capacity < static_cast<long long>(L.total)) {
+        return fail(ctx, WOS_ERR_INVALID, "wos_scene_arena: buffer too small");
+    }
+    cudaSetDevice(ctx->device);
+    WOS_CUDA(ctx, cudaMemcpyAsync(out, ctx->sdev.arena.ptr, L.total, cudaMemcpyDeviceToHost,
+                                  ctx->stream), "D2H");
+    WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "scene arena");
+    return WOS_OK;
 }
 
 extern "C" int wos_load_obj(wos_context *ctx, const char *path, int leaf_size) {

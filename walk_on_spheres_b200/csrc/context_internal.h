@@ -19,6 +19,18 @@ struct DeviceBuffer {
     void release();
 };
 
+// Where each array of a scene lives in its arena (one device allocation):
+// box64, seg64, segid, tri64, wbox, wprim, wide2bin, the wide tree's height
+// offsets and slot_verts, each at a 256-byte aligned offset.  The sizes
+// follow from the scene's metadata alone.
+struct ArenaLayout {
+    static constexpr int kParts = 9;
+    size_t offset[kParts];
+    size_t bytes[kParts];
+    size_t total;
+};
+ArenaLayout arena_layout(const HostScene &meta);
+
 // Device copy of one HostScene (all tree and primitive arrays) and the
 // views the kernels take.
 struct SceneDevice {
@@ -31,12 +43,22 @@ struct SceneDevice {
     // wait: later work on `stream` is ordered after them) and fills view /
     // wide.
     cudaError_t upload(const HostScene &h, cudaStream_t stream);
+    // The same arena built on the device from the mesh alone (`meta` from
+    // scene_meta: no host arrays), bit-identical to upload(build_scene(...)),
+    // then its lattice; enqueued on `stream` (scene_build_gpu.cu).
+    cudaError_t build_on_device(const HostScene &meta, cudaStream_t stream);
+    // view / wide / slot_verts over the arena of a scene with this metadata.
+    void set_views(const HostScene &meta);
     // Builds the FAST_FP32 distance lattice into `lattice` and wide.gd.
     cudaError_t build_lattice(const HostScene &h, cudaStream_t stream);
     void release();
 };
 
 double effective_epsilon(const wos_params &p);
+
+// Where trees are built: on the device (default) or, with
+// WOS_TREE_BUILD=host, on the host threads; both give the same arrays.
+bool device_tree_build();
 
 // Argument checks shared by the grid entry points: an empty string when
 // `p` (against the context's mesh) or the grid is acceptable, else the

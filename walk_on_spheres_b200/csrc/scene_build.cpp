@@ -276,18 +276,14 @@ static void slab_of(const std::vector<double> &pts, int dim, double *n, double &
     }
 }
 
+void wide_layout(HostScene &sc);
+
 static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
     const int n = sc.n_prims;
-    int H = 1;
-    long long span = 32;
-    while (span < n) {
-        span *= 32;
-        ++H;
-    }
-    sc.wH = H;
+    wide_layout(sc);
+    const int H = sc.wH;
     WideBuilder W{dim, items};
     W.node(0, n, H);
-    sc.w_npad = (n + 31) / 32 * 32;
 
     // binary slot of every primitive (for the FP64 records)
     std::vector<int> bin_of(n);
@@ -324,14 +320,9 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
     }
     // heights 1..H-1 are children of some node.  Children of one parent form
     // a group block of nbox x 32 floats (field f of child k at f*32 + k):
-    // box lo[dim], hi[dim], slab normal[dim], slab offset, half-thickness.
+    // box lo[dim], hi[dim], slab normal[dim], slab offset, half-thickness
+    // (offsets w_off and size w_box_total from wide_layout).
     const int nbox = nc + dim + 2;
-    int total = 0;
-    for (int h = 1; h < H; ++h) {
-        sc.w_off[h] = total;
-        total += static_cast<int>(cnt[h + 1]) * nbox * 32;
-    }
-    sc.w_box_total = std::max(total, nbox * 32);
     const double widen = std::ldexp(sc.scale, -20);
     sc.wbox.assign(static_cast<size_t>(sc.w_box_total), 0.0f);
     // padding children are empty boxes (lo = +inf, hi = -inf) with an
@@ -452,6 +443,64 @@ std::string check_mesh(int dim, const double *verts, int n_verts, const int *pri
     return std::string();
 }
 
+void wide_layout(HostScene &sc) {
+    const int n = sc.n_prims, dim = sc.dim;
+    int H = 1;
+    long long span = 32;
+    while (span < n) {
+        span *= 32;
+        ++H;
+    }
+    sc.wH = H;
+    sc.w_npad = (n + 31) / 32 * 32;
+    std::vector<long long> cnt(H + 1);
+    cnt[0] = n;
+    for (int h = 1; h <= H; ++h) cnt[h] = (cnt[h - 1] + 31) / 32;
+    const int nbox = 2 * dim + dim + 2;
+    int total = 0;
+    for (int h = 0; h < 8; ++h) sc.w_off[h] = 0;
+    for (int h = 1; h < H; ++h) {
+        sc.w_off[h] = total;
+        total += static_cast<int>(cnt[h + 1]) * nbox * 32;
+    }
+    sc.w_box_total = std::max(total, nbox * 32);
+}
+
+std::string scene_meta(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                       const int *boundary_ids, int leaf_size, HostScene &sc) {
+    std::string err = check_mesh(dim, verts, n_verts, prims, n_prims, leaf_size);
+    if (!err.empty()) return err;
+    if (leaf_size == 0) leaf_size = 4;
+    sc = HostScene{};
+    sc.dim = dim;
+    sc.n_prims = n_prims;
+    sc.n_verts = n_verts;
+    sc.leaf_size = leaf_size;
+    sc.verts.assign(verts, verts + static_cast<size_t>(n_verts) * dim);
+    sc.prims.assign(prims, prims + static_cast<size_t>(n_prims) * dim);
+    sc.boundary_ids.assign(n_prims, 0);
+    if (dim == 2 && boundary_ids) sc.boundary_ids.assign(boundary_ids, boundary_ids + n_prims);
+    auto V = [&](int v, int k) { return verts[static_cast<size_t>(dim) * v + k]; };
+    for (int k = 0; k < 3; ++k) {
+        sc.bbox[2 * k] = k < dim ? V(0, k) : 0.0;
+        sc.bbox[2 * k + 1] = sc.bbox[2 * k];
+    }
+    for (int v = 1; v < n_verts; ++v) {
+        for (int k = 0; k < dim; ++k) {
+            const double x = V(v, k);
+            if (x < sc.bbox[2 * k]) sc.bbox[2 * k] = x;
+            else if (x > sc.bbox[2 * k + 1]) sc.bbox[2 * k + 1] = x;
+        }
+    }
+    sc.scale = std::max({1.0, sc.bbox[1] - sc.bbox[0], sc.bbox[3] - sc.bbox[2],
+                         sc.bbox[5] - sc.bbox[4]});
+    int D = 0;
+    while (((static_cast<long long>(n_prims) + (1ll << D) - 1) >> D) > leaf_size) ++D;
+    sc.depth = D;
+    wide_layout(sc);
+    return std::string();
+}
+
 std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                         const int *boundary_ids, int leaf_size, HostScene &sc) {
     if (dim != 2 && dim != 3) return "mesh dimension must be 2 or 3";
@@ -506,10 +555,13 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
             const int a = prims[2 * p], b = prims[2 * p + 1];
             const double dx = V(b, 0) - V(a, 0), dy = V(b, 1) - V(a, 1);
             if (!(dx * dx + dy * dy > 0.0)) return "mesh contains a zero-length line segment";
+            // "+ 0.0" turns -0.0 into +0.0: the boxes' min / max then do not
+            // depend on the order items are visited in (the device build
+            // visits them in another order)
             for (int k = 0; k < 2; ++k) {
-                it.lo[k] = std::fmin(V(a, k), V(b, k));
-                it.hi[k] = std::fmax(V(a, k), V(b, k));
-                it.c[k] = (V(a, k) + V(b, k)) / 2.0;
+                it.lo[k] = std::fmin(V(a, k), V(b, k)) + 0.0;
+                it.hi[k] = std::fmax(V(a, k), V(b, k)) + 0.0;
+                it.c[k] = (V(a, k) + V(b, k)) / 2.0 + 0.0;
             }
         } else {
             const int a = prims[3 * p], b = prims[3 * p + 1], c = prims[3 * p + 2];
@@ -519,9 +571,9 @@ std::string build_scene(int dim, const double *verts, int n_verts, const int *pr
                          cz = abx * acy - aby * acx;
             if (!(cx * cx + cy * cy + cz * cz > 0.0)) return "mesh contains a degenerate triangle";
             for (int k = 0; k < 3; ++k) {
-                it.lo[k] = std::fmin(std::fmin(V(a, k), V(b, k)), V(c, k));
-                it.hi[k] = std::fmax(std::fmax(V(a, k), V(b, k)), V(c, k));
-                it.c[k] = (V(a, k) + V(b, k) + V(c, k)) / 3.0;
+                it.lo[k] = std::fmin(std::fmin(V(a, k), V(b, k)), V(c, k)) + 0.0;
+                it.hi[k] = std::fmax(std::fmax(V(a, k), V(b, k)), V(c, k)) + 0.0;
+                it.c[k] = (V(a, k) + V(b, k) + V(c, k)) / 3.0 + 0.0;
             }
         }
     }

@@ -55,4 +55,10 @@ unsigned host_threads();
 std::string build_scene(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
                         const int *boundary_ids, int leaf_size, HostScene &out);
 
+// The checks of build_scene and everything of the scene but its arrays:
+// the mesh itself, bounding box, scale, binary-tree depth and the 32-wide
+// tree's layout (wH, w_npad, w_off, w_box_total), for a build on the device.
+std::string scene_meta(int dim, const double *verts, int n_verts, const int *prims, int n_prims,
+                       const int *boundary_ids, int leaf_size, HostScene &out);
+
 }  // namespace wosb
