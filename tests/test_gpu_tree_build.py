@@ -58,6 +58,36 @@ MESHES = {
 }
 
 
+PARTS = ("box64", "seg64", "segid", "tri64", "wbox", "wprim", "wide2bin", "offsets",
+         "slot_verts")
+
+
+def _parts(mesh, leaf):
+    """(name, start, end) of each array in the scene arena (arena_layout)."""
+    n, dim = mesh.n_prims, mesh.dim
+    leaf = leaf or 4
+    D = 0
+    while -(-n // (1 << D)) > leaf:
+        D += 1
+    H, span = 1, 32
+    while span < n:
+        span, H = span * 32, H + 1
+    cnt = [n]
+    for _ in range(H):
+        cnt.append(-(-cnt[-1] // 32))
+    nbox = 3 * dim + 2
+    total = sum(cnt[h + 1] * nbox * 32 for h in range(1, H))
+    npad = -(-n // 32) * 32
+    sizes = [(1 << (D + 1)) * 2 * dim * 8, n * 32 if dim == 2 else 0, n * 8 if dim == 2 else 0,
+             n * 112 if dim == 3 else 0, max(total, nbox * 32) * 4,
+             npad * (5 if dim == 2 else 16) * 4, npad * 4, 32, n * dim * 4]
+    out, at = [], 0
+    for name, b in zip(PARTS, sizes):
+        out.append((name, at, at + b))
+        at += -(-max(b, 16) // 256) * 256
+    return out
+
+
 @pytest.fixture
 def host_build():
     def set_host(flag: bool):
@@ -81,7 +111,8 @@ def test_device_build_is_byte_identical(solver, host_build, name, leaf):
     dev = _arena(solver)
     assert host.size == dev.size
     diff = np.flatnonzero(host != dev)
-    assert diff.size == 0, f"{diff.size} bytes differ, first at {diff[:8]}"
+    where = {name: int(((diff >= a) & (diff < b)).sum()) for name, a, b in _parts(mesh, leaf)}
+    assert diff.size == 0, f"{diff.size} bytes differ: {where}"
 
 
 @pytest.mark.parametrize("name", ["circle1024", "sphere16128"])

@@ -729,6 +729,10 @@ cudaError_t SceneDevice::build_on_device(const HostScene &m, cudaStream_t stream
         }
         if ((r = cudaMemcpyAsync(offs, m.w_off, 8 * sizeof(int), cudaMemcpyHostToDevice,
                                  stream)) != cudaSuccess) return r;
+        // the permutations start as valid indices (0), whatever a kernel misses
+        for (int *perm : {order, witem, bin_of}) {
+            if ((r = cudaMemsetAsync(perm, 0, nn * sizeof(int), stream)) != cudaSuccess) return r;
+        }
         items_kernel<<<blocks_for(n), 256, 0, stream>>>(dim, d_verts, d_prims, n, it);
         // one list per axis, sorted by (centroid, primitive id): a stable
         // radix sort of the centroid keys over the primitives in id order
@@ -777,8 +781,8 @@ cudaError_t SceneDevice::build_on_device(const HostScene &m, cudaStream_t stream
             if ((r = split_level(g, 1 << l, box64, l, l < D)) != cudaSuccess) return r;
         }
         const int leaves = 1 << D;
-        group_sort_kernel<<<blocks_for(leaves), 128, 0, stream>>>(1, D, n, leaves, lists[0],
-                                                                  order);
+        group_sort_kernel<<<blocks_for(leaves, 128), 128, 0, stream>>>(1, D, n, leaves,
+                                                                       lists[0], order);
         if (dim == 2) {
             records2_kernel<<<blocks_for(n), 256, 0, stream>>>(d_verts, d_prims, d_bids, order,
                                                                n, seg64, segid, rec32, inv32,
@@ -804,8 +808,8 @@ cudaError_t SceneDevice::build_on_device(const HostScene &m, cudaStream_t stream
             done += rd.size();
         }
         const int clusters = (n + 31) / 32;
-        group_sort_kernel<<<blocks_for(clusters), 128, 0, stream>>>(0, 0, n, clusters, lists[0],
-                                                                    witem);
+        group_sort_kernel<<<blocks_for(clusters, 128), 128, 0, stream>>>(0, 0, n, clusters,
+                                                                         lists[0], witem);
         inverse_kernel<<<blocks_for(n), 256, 0, stream>>>(order, n, bin_of);
         wide2bin_kernel<<<blocks_for(m.w_npad), 256, 0, stream>>>(witem, bin_of, n, m.w_npad,
                                                                   wide2bin);
