@@ -88,14 +88,17 @@ METHOD_NAMES = {"fast": "FAST_FP32 (FP32 walk + FP64 epsilon shell, FP64 sums)",
 # The reference arm's slices: step s solves the grid points whose linear
 # index is congruent to s modulo REF_STRIDE.
 REF_STRIDE = 128
-# Per walk step of walk_fast_kernel on this workload (FAST_FP32), from one
-# ncu capture of each source mode's launch (`python -m
-# walk_on_spheres_b200.benchmarks --profile disk_uniform` / `disk_green`):
-# warp instructions issued (sm__inst_issued.sum), L2 bytes (lts__t_bytes.sum)
-# and DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum), each divided
-# by the launch's walk steps, and the L2 peak ncu reports for the part.
-NCU_PER_STEP = {"uniform": {"issued": None, "l2_bytes": None, "dram_bytes": None},
-                "green": {"issued": None, "l2_bytes": None, "dram_bytes": None}}
+# walk_fast_kernel on this workload (FAST_FP32), from one ncu capture of each
+# source mode's launch (`python -m walk_on_spheres_b200.benchmarks --profile
+# disk_uniform` / `disk_green`, 512 walks): warp instructions issued
+# (sm__inst_issued.sum) and L2 bytes (lts__t_bytes.sum) per walk step, DRAM
+# bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch (the
+# distance lattice read once and the fields written: the same at any walk
+# count), and the L2 peak the capture implies (lts__t_bytes.sum.per_second
+# over lts__t_sectors.sum.pct_of_peak_sustained_elapsed).
+NCU_PER_STEP = {"uniform": {"issued": None, "l2_bytes": None},
+                "green": {"issued": None, "l2_bytes": None}}
+NCU_DRAM_BYTES_PER_LAUNCH = None
 NCU_L2_PEAK_GBS = None
 ISSUE_SLOTS_PER_SM_CYCLE = 4   # one warp instruction per SM sub-partition per cycle
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
@@ -275,11 +278,11 @@ def roofline(per_mode: dict, clock_mhz: float | None, sms: int, launches: int) -
         return out
     issued = sum(NCU_PER_STEP[m]["issued"] * st for m, (_, st) in per_mode.items())
     l2 = sum(NCU_PER_STEP[m]["l2_bytes"] * st for m, (_, st) in per_mode.items())
-    dram = sum(NCU_PER_STEP[m]["dram_bytes"] * st for m, (_, st) in per_mode.items())
+    dram = NCU_DRAM_BYTES_PER_LAUNCH * launches
     out["achieved"] = issued / secs / 1e9
     if out["peak"]:
         out["frac"] = out["achieved"] / out["peak"]
-    out["traffic"] = dram / launches
+    out["traffic"] = NCU_DRAM_BYTES_PER_LAUNCH
     out["per_step"] = {m: dict(NCU_PER_STEP[m]) for m in per_mode}
     out["memory"] = {
         "l2_gbs": l2 / secs / 1e9, "l2_peak_gbs": NCU_L2_PEAK_GBS,

@@ -259,6 +259,20 @@ int wos_batch::plan() {
     auto *part = static_cast<TaskPartial *>(partials.ptr);
     auto *ctr = static_cast<DeviceCounters *>(counters.ptr);
     items.assign(n, BatchItem{});
+    // near-boundary lists of each mesh, for the largest threshold among its
+    // FAST_FP32 solves (the walks read the lists' pointers from the items)
+    std::vector<float> list_t(meshes.size(), 0.0f);
+    for (const BatchSolve &b : solves) {
+        if (b.p.method != WOS_METHOD_FAST_FP32) continue;
+        const BatchMesh &m = *meshes[b.mesh];
+        list_t[b.mesh] = std::max(list_t[b.mesh],
+                                  near_list_threshold(m.dev.wide, effective_epsilon(b.p),
+                                                      std::ldexp(m.scene.scale, -16)));
+    }
+    for (size_t k = 0; k < meshes.size(); ++k) {
+        WOS_CUDA(ctx, meshes[k]->dev.ensure_lists(list_t[k], ctx->sms, ctx->stream),
+                 "near-boundary lists");
+    }
     families.clear();
     for (int i = 0; i < n; ++i) {
         const BatchSolve &b = solves[order[i]];

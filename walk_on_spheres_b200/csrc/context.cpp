@@ -179,7 +179,55 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
     return build_lattice(h, stream);
 }
 
+cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
+    if (wide.gd == nullptr || !(t > 0.0f)) return cudaSuccess;
+    if (const char *env = std::getenv("WOS_NEAR_LISTS")) {
+        if (std::string(env) == "0") return cudaSuccess;
+    }
+    if (wide.gl != nullptr && list_built >= t) return cudaSuccess;
+    const float tb = t * 1.25f;
+    const size_t nodes = static_cast<size_t>(wide.gn[0]) * wide.gn[1] * wide.gn[2];
+    cudaError_t e = glist.reserve(nodes * sizeof(int));
+    if (e != cudaSuccess) return e;
+    if ((e = gcount.reserve(2 * sizeof(unsigned))) != cudaSuccess) return e;
+    auto *count = static_cast<unsigned *>(gcount.ptr);
+    if ((e = launch_near_band(wide, tb, count, stream)) != cudaSuccess) return e;
+    unsigned band = 0;
+    if ((e = cudaMemcpyAsync(&band, count, sizeof(band), cudaMemcpyDeviceToHost, stream)) !=
+        cudaSuccess) {
+        return e;
+    }
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    WideView w = wide;
+    w.gk = near_list_capacity(w.dim);
+    if (const char *env = std::getenv("WOS_NEAR_CAPACITY")) {
+        const int k = std::atoi(env);
+        if (k >= 1 && k <= 32) w.gk = k;
+    }
+    if ((e = gpool.reserve(std::max<size_t>(band, 1) * w.gk * sizeof(int))) != cudaSuccess) {
+        return e;
+    }
+    // a point is within r_max of its nearest node; 8 lattice margins cover
+    // the FP32 rounding of the distances
+    const double rmax = 0.5 * w.gh * std::sqrt(static_cast<double>(w.dim)) * (1.0 + 1e-3);
+    const float extra = static_cast<float>(2.0 * rmax + 8.0 * lattice_margin);
+    if ((e = launch_near_lists(w, tb, extra, static_cast<int *>(glist.ptr),
+                               static_cast<int *>(gpool.ptr), static_cast<int>(band), count + 1,
+                               sms, stream)) != cudaSuccess) {
+        return e;
+    }
+    if ((e = gaos.reserve(prim_aos_bytes(w))) != cudaSuccess) return e;
+    if ((e = launch_prim_aos(w, static_cast<float *>(gaos.ptr), stream)) != cudaSuccess) return e;
+    wide.gk = w.gk;
+    wide.gl = static_cast<const int *>(glist.ptr);
+    wide.gpool = static_cast<const int *>(gpool.ptr);
+    wide.aos = static_cast<const float4 *>(gaos.ptr);
+    list_built = tb;
+    return cudaSuccess;
+}
+
 void SceneDevice::set_views(const HostScene &h) {
+    list_built = -1.0f;
     const ArenaLayout L = arena_layout(h);
     auto *base = static_cast<char *>(arena.ptr);
     auto at = [&](int k) { return static_cast<const void *>(base + L.offset[k]); };
@@ -235,6 +283,7 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
     wide.ginv = static_cast<float>(1.0 / step);
     // FP32 primitive distances carry a few ulps of the largest coordinate
     const float margin = static_cast<float>(4e-6 * std::max(mag, ext));
+    lattice_margin = margin;
     const size_t count = static_cast<size_t>(n[0]) * n[1] * n[2];
     cudaError_t e = lattice.reserve(sizeof(float) * count);
     if (e != cudaSuccess) return e;
@@ -270,6 +319,11 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
 void SceneDevice::release() {
     arena.release();
     lattice.release();
+    glist.release();
+    gpool.release();
+    gcount.release();
+    gaos.release();
+    list_built = -1.0f;
     slot_verts = nullptr;
 }
 
@@ -404,6 +458,12 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     const double eps = effective_epsilon(p);
     // boundary tolerance 1e-10 * max(1, mesh extents), include/wos/runner.hpp:86-88
     const double btol = 1e-10 * scene.scale;
+    if (p.method == WOS_METHOD_FAST_FP32) {
+        // near-boundary lists for this epsilon (one-time set-up per mesh)
+        const float t = near_list_threshold(sdev.wide, eps, std::ldexp(scene.scale, -16));
+        WOS_CUDA(this, sdev.ensure_lists(t, sms, stream), "near-boundary lists");
+        wide = sdev.wide;
+    }
     auto *loc = static_cast<uint8_t *>(location.ptr);
     auto *st = static_cast<StartRecord *>(start.ptr);
     auto *ctr = static_cast<DeviceCounters *>(counters.ptr);

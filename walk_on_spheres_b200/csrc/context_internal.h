@@ -49,6 +49,15 @@ struct SceneDevice {
     cudaError_t build_on_device(const HostScene &meta, cudaStream_t stream);
     // view / wide / slot_verts over the arena of a scene with this metadata.
     void set_views(const HostScene &meta);
+
+    // Near-boundary candidate lists (wide.gl / gpool): built for every
+    // lattice node with value up to 1.25 t, unless lists covering t exist;
+    // a scene without a lattice, or WOS_NEAR_LISTS=0, has none.  Waits for
+    // the stream once (the band size sizes the list pool).
+    cudaError_t ensure_lists(float t, int sms, cudaStream_t stream);
+    DeviceBuffer glist, gpool, gcount, gaos;
+    float list_built = -1.0f;  // the value up to which lists were built
+    float lattice_margin = 0.0f;
     // Builds the FAST_FP32 distance lattice into `lattice` and wide.gd.
     cudaError_t build_lattice(const HostScene &h, cudaStream_t stream);
     void release();

@@ -57,12 +57,25 @@ struct WideView {
     // D >= gratio * r, i.e. when it is at least (gratio - 1) / (gratio + 1)
     // of the upper bound D + r of the true distance
     float gratio;
+    // Near-boundary candidate lists (null when absent): gl[node] is -1 or
+    // the index of the node's list, gk wide slots at gpool + gl[node] * gk
+    // (-1 past its end).  The list holds every primitive within
+    // d(node) + 2 r_max of the node (r_max the largest distance from a point
+    // to its nearest node), so it holds the nearest primitive of every point
+    // whose nearest node this is.
+    const int *gl;
+    const int *gpool;
+    int gk;
+    // the primitive records again, one per wide slot, contiguous (2D: 5 of 8
+    // floats, 3D: 16 floats), for the list scans' per-lane gathers
+    const float4 *aos;
 };
 
 // Lattice value D at the node nearest to p and the distance r from p to it:
 // D - r <= d(p) <= D + r (up to D's downward rounding).
 struct LatticeSample {
     float d, r;
+    int node;  // lattice index of the node
 };
 
 template <int DIM>
@@ -73,13 +86,15 @@ __device__ __forceinline__ LatticeSample lattice_sample(const WideView &w, float
     const float dx = px - (w.glo[0] + static_cast<float>(i) * w.gh);
     const float dy = py - (w.glo[1] + static_cast<float>(j) * w.gh);
     if (DIM == 2) {
-        const float d = __ldg(w.gd + static_cast<long long>(i) * w.gn[1] + j);
-        return LatticeSample{d, sqrtf(dx * dx + dy * dy)};
+        const int node = i * w.gn[1] + j;
+        const float d = __ldg(w.gd + node);
+        return LatticeSample{d, sqrtf(dx * dx + dy * dy), node};
     }
     const int k = min(max(__float2int_rn((pz - w.glo[2]) * w.ginv), 0), w.gn[2] - 1);
     const float dz = pz - (w.glo[2] + static_cast<float>(k) * w.gh);
-    const float d = __ldg(w.gd + (static_cast<long long>(i) * w.gn[1] + j) * w.gn[2] + k);
-    return LatticeSample{d, sqrtf(dx * dx + dy * dy + dz * dz)};
+    const int node = (i * w.gn[1] + j) * w.gn[2] + k;
+    const float d = __ldg(w.gd + node);
+    return LatticeSample{d, sqrtf(dx * dx + dy * dy + dz * dz), node};
 }
 
 // Lower bound of the boundary distance at p from the nearest lattice node.
@@ -173,6 +188,88 @@ __device__ __forceinline__ WideResult lane_nearest(const WideView &w, float px, 
         }
     }
     return WideResult{best, slot};
+}
+
+// Closest primitive among a near-boundary candidate list (at most k wide
+// slots, -1 past the end), found by this lane alone; the first minimum in
+// list order wins.
+template <int DIM>
+__device__ __forceinline__ WideResult list_nearest(const WideView &w, const int *list, int k,
+                                                   float px, float py, float pz) {
+    float best = INFINITY;
+    int slot = -1;
+    for (int q = 0; q < k; ++q) {
+        const int s = __ldg(list + q);
+        if (s < 0) break;
+        float d2;
+        if (DIM == 2) {
+            const float4 a = __ldg(w.aos + 2 * s);
+            const float inv = __ldg(reinterpret_cast<const float *>(w.aos + 2 * s + 1));
+            const float wx = px - a.x, wy = py - a.y;
+            const float t = fminf(fmaxf((wx * a.z + wy * a.w) * inv, 0.0f), 1.0f);
+            const float dx = wx - t * a.z, dy = wy - t * a.w;
+            d2 = dx * dx + dy * dy;
+        } else {
+            float4 rec[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) rec[f] = __ldg(w.aos + 4 * s + f);
+            d2 = eberly32(px, py, pz, rec);
+        }
+        if (d2 < best) {
+            best = d2;
+            slot = s;
+        }
+    }
+    return WideResult{best, slot};
+}
+
+// Every primitive within squared FP32 distance r2 of (px, py, pz), found by
+// the whole warp (all lanes call it with the same point): the wide slots in
+// ascending order go to out[0 .. cap), the count (which may exceed cap) is
+// returned to every lane.  Children are visited when their lower bound
+// (box and slab) is within r2.
+template <int DIM>
+__device__ int wide_range(const WideView &w, float px, float py, float pz, float r2, int *out,
+                          int cap) {
+    constexpr unsigned kAll = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    int count = 0;
+    auto leaf = [&](int cluster) {
+        const float d2 = wide_prim_dist<DIM>(w, cluster, px, py, pz);
+        const unsigned m = __ballot_sync(kAll, d2 <= r2);
+        const int at = count + __popc(m & below);
+        if (((m >> lane) & 1u) && at < cap) out[at] = cluster * 32 + static_cast<int>(lane);
+        count += __popc(m);
+    };
+    if (w.H == 1) {
+        leaf(0);
+        return count;
+    }
+    // mask[h]: children of height h (of the node parent[h]) still to visit
+    unsigned mask[8];
+    int parent[8];
+    int h = w.H - 1;
+    parent[h] = 0;
+    mask[h] = __ballot_sync(kAll, wide_box_dist<DIM>(w, h, 0, px, py, pz) <= r2);
+    for (;;) {
+        if (mask[h] == 0u) {
+            if (h == w.H - 1) break;
+            ++h;
+            continue;
+        }
+        const int k = __ffs(mask[h]) - 1;
+        mask[h] &= mask[h] - 1u;
+        const int child = parent[h] * 32 + k;
+        if (h == 1) {
+            leaf(child);
+        } else {
+            --h;
+            parent[h] = child;
+            mask[h] = __ballot_sync(kAll, wide_box_dist<DIM>(w, h, child, px, py, pz) <= r2);
+        }
+    }
+    return count;
 }
 
 // Traversal classes: a kernel compiled for one class carries only that

@@ -18,6 +18,12 @@ int wos_context::run_heat(const wos_params &p, const HeatDesc &h, const PointSet
                           HeatOut out, wos_counters *counters_out) {
     cudaSetDevice(device);
     const long long n = ps.n;
+    if (p.method == WOS_METHOD_FAST_FP32) {
+        // near-boundary lists for this epsilon (one-time set-up per mesh)
+        const float t = near_list_threshold(sdev.wide, p.epsilon, std::ldexp(scene.scale, -16));
+        WOS_CUDA(this, sdev.ensure_lists(t, sms, stream), "near-boundary lists");
+        wide = sdev.wide;
+    }
     WOS_CUDA(this, location.reserve(std::max<long long>(n, 1)), "alloc location");
     WOS_CUDA(this, start.reserve(sizeof(StartRecord) * std::max<long long>(n, 1)), "alloc start");
     WOS_CUDA(this, counters.reserve(sizeof(DeviceCounters)), "alloc counters");

@@ -62,6 +62,8 @@ struct FastArgs {
     float shrink;   // 1 - tau: conservative radius factor
     float exact2;   // below this squared distance the FP32 query prunes exactly
     float shell2;   // (eps + shell_delta)^2: FP32 radius inside the epsilon shell
+    float list_t;   // nodes with lattice value <= list_t answer queries from their
+                    // candidate list (near_list_threshold; -1: no lists)
     int chunk;
     int chunks;
     long long n_tasks;
@@ -193,6 +195,37 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
 // (rows within `tol` of an edge or vertex stay unclassified), store 0 without
 // a query.
 size_t lattice_skip_bytes(const WideView &w);
+
+// Lattice value below which a walk step of a solve with this epsilon may run
+// a closest-point query: above it, for any point whose nearest node has that
+// value, the lattice step is taken (D >= gratio r and (D - r)(1 - tau) beyond
+// the shell for every r <= r_max).  Near-boundary lists are needed below it.
+inline float near_list_threshold(const WideView &w, double epsilon, double shell_delta) {
+    const double tau = 1.0 / 1024.0;
+    const double rmax = 0.5 * w.gh * (w.dim == 3 ? 1.7320508075688772 : 1.4142135623730951) *
+                        (1.0 + 1e-3);
+    const double shell = epsilon + shell_delta;
+    const double a = w.gratio * rmax, b = shell / (1.0 - tau) + rmax;
+    return static_cast<float>((a > b ? a : b) * (1.0 + 1e-3));
+}
+
+// Capacity of a near-boundary list (wide slots).
+// (16 in 2D and 3D: on the B200 16, 24 and 32 ran within 1% of each other,
+// 8 cost the heat walks 1.7x)
+inline int near_list_capacity(int) { return 16; }
+
+// Near-boundary candidate lists of a lattice (w's lattice built): every node
+// with 0 <= value <= t gets the wide slots of all primitives within its exact
+// FP32 distance plus `extra` (2 r_max and a rounding margin), if there are
+// at most near_list_capacity of them.  `count` (device) receives the number
+// of such nodes first (band pass, pool null), then the lists are written.
+cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaStream_t stream);
+// The primitive records one slot after another (WideView::aos) for the list
+// scans: prim_aos_bytes(w) bytes.
+size_t prim_aos_bytes(const WideView &w);
+cudaError_t launch_prim_aos(const WideView &w, float *aos, cudaStream_t stream);
+cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
+                              int pool_lists, unsigned *counter, int sms, cudaStream_t stream);
 cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin, float *out,
                              int sms, void *scratch, double tol, cudaStream_t stream);
 // lattice_bound at each point (FP32), NaN where the scene has no lattice.

@@ -56,6 +56,7 @@ struct HeatArgs {
     double eps;
     int max_steps;
     float keep, shrink, exact2, shell2;  // FP32 query bounds (see kernels_fast.cu)
+    float list_t;                        // near-boundary lists below this value (-1: none)
     int chunk;
     int chunks;
     long long n_tasks;
@@ -282,6 +283,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
         while (__any_sync(kFull, active)) {
             bool done = false;
             bool need_query = false;
+            bool listed = false;  // answered from a near-boundary list
             double value = 0.0;
             if (active) {
                 bool stop = false;
@@ -350,6 +352,21 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                             if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
                                 R = gb;
                                 need_query = false;
+                            } else if (ls.d <= a.list_t) {
+                                // near the boundary: this lane's own query over
+                                // the node's candidate list, when it has one
+                                const int li = __ldg(wv.gl + ls.node);
+                                if (li >= 0) {
+                                    const WideResult q = list_nearest<DIM>(
+                                        wv, wv.gpool + static_cast<long long>(li) * wv.gk, wv.gk,
+                                        static_cast<float>(p.x), static_cast<float>(p.y),
+                                        static_cast<float>(p.z));
+                                    const float r = sqrtf(q.best);
+                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                    slot = q.slot;
+                                    need_query = false;
+                                    listed = true;
+                                }
                             }
                         }
                     } else {
@@ -364,7 +381,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
             }
             if constexpr (kF32) {
                 unsigned pending = __ballot_sync(kFull, need_query);
-                queries += __popc(pending);
+                queries += __popc(pending) + __popc(__ballot_sync(kFull, listed));
                 float qbest = 0.0f;
                 int qslot = -1;
                 while (pending) {
@@ -616,6 +633,7 @@ cudaError_t launch_heat(const SceneView &s, const WideView &w, const PointSet &p
     a.shrink = static_cast<float>(1.0 - tau);
     a.shell2 = static_cast<float>(shell * shell);
     a.exact2 = static_cast<float>(shell * shell / ((1.0 - tau) * (1.0 - tau)));
+    a.list_t = w.gl != nullptr ? near_list_threshold(w, epsilon, shell_delta) : -1.0f;
     a.chunk = plan.chunk;
     a.chunks = plan.chunks;
     a.n_tasks = plan.n_tasks;

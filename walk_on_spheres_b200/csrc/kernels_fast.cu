@@ -76,6 +76,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     while (__any_sync(kFull, active)) {
         bool done = false;
         bool need_query = false;
+        bool listed = false;  // answered from a near-boundary list
         double value = 0.0;
         if (active) {
             bool stop = false;
@@ -148,6 +149,21 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                             if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
                                 R = gb;
                                 need_query = false;
+                            } else if (ls.d <= a.list_t) {
+                                // near the boundary: this lane's own query over
+                                // the node's candidate list, when it has one
+                                const int li = __ldg(wv.gl + ls.node);
+                                if (li >= 0) {
+                                    const WideResult q = list_nearest<DIM>(
+                                        wv, wv.gpool + static_cast<long long>(li) * wv.gk, wv.gk,
+                                        static_cast<float>(p.x), static_cast<float>(p.y),
+                                        static_cast<float>(p.z));
+                                    const float r = sqrtf(q.best);
+                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                    slot = q.slot;
+                                    need_query = false;
+                                    listed = true;
+                                }
                             }
                         }
                     }
@@ -175,7 +191,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         } else if constexpr (kF32) {
             // the warp resolves every pending closest-point query together
             unsigned pending = __ballot_sync(kFull, need_query);
-            queries += __popc(pending);
+            queries += __popc(pending) + __popc(__ballot_sync(kFull, listed));
             float qbest = 0.0f;
             int qslot = -1;
             while (pending) {
@@ -654,7 +670,8 @@ __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin
                 }
             }
             if (__all_sync(kFull, out_n)) {
-                if (lane == 0) out[t] = 0.0f;
+                // -0.0: a valid bound that marks the node as skipped
+                if (lane == 0) out[t] = -0.0f;
                 continue;
             }
         }
@@ -685,23 +702,22 @@ __device__ __forceinline__ void add_crossing(unsigned *count, float *cross, long
     if (c < static_cast<unsigned>(kRowCrossings)) cross[row * kRowCrossings + c] = x;
 }
 
-// 2D: one thread per segment, rows y_j = glo[1] + j h.
-__global__ void row_crossings2_kernel(SceneView s, WideView w, double tol, unsigned *count,
-                                      float *cross) {
+// 2D: one thread per segment, rows y_j = glo[1] + j h.  A segment crosses a
+// row when min(y) <= y_j < max(y): adjacent segments share their endpoint's
+// exact coordinates, so a row through a vertex counts the crossing once (or
+// twice at a turning point) and the parity stays right.
+__global__ void row_crossings2_kernel(SceneView s, WideView w, unsigned *count, float *cross) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= s.n_prims) return;
     const double2 a = s.seg64[2 * p], b = s.seg64[2 * p + 1];
     const double ylo = fmin(a.y, b.y), yhi = fmax(a.y, b.y);
+    if (!(ylo < yhi)) return;  // horizontal: never crosses under the half-open rule
     const double h = w.gh, y0 = w.glo[1];
-    const int j0 = max(0, static_cast<int>(floor((ylo - tol - y0) / h)));
-    const int j1 = min(w.gn[1] - 1, static_cast<int>(ceil((yhi + tol - y0) / h)));
+    const int j0 = max(0, static_cast<int>(floor((ylo - y0) / h)) - 1);
+    const int j1 = min(w.gn[1] - 1, static_cast<int>(ceil((yhi - y0) / h)) + 1);
     for (int j = j0; j <= j1; ++j) {
         const double y = static_cast<double>(w.glo[1] + static_cast<float>(j) * w.gh);
-        if (y < ylo - tol || y > yhi + tol) continue;
-        if (fabs(y - a.y) <= tol || fabs(y - b.y) <= tol) {
-            atomicOr(count + j, kRowUnknown);
-            continue;
-        }
+        if (!(ylo <= y && y < yhi)) continue;
         const double x = a.x + (y - a.y) * (b.x - a.x) / (b.y - a.y);
         add_crossing(count, cross, j, static_cast<float>(x));
     }
@@ -814,6 +830,118 @@ __global__ void lattice_bounds_kernel(WideView w, const double *pts, long long n
 }
 }  // namespace
 
+namespace {
+// Lattice nodes in the near-boundary band: value in [0, t] (-0.0 marks a
+// skipped node).
+__global__ void near_band_kernel(const float *__restrict__ gd, long long n, float t,
+                                 unsigned *count) {
+    unsigned c = 0;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += stride) {
+        const float d = gd[i];
+        c += (!signbit(d) && d <= t) ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+// One band node per warp: its exact FP32 distance d, then every primitive
+// within d + extra, kept as its list when there are at most K.
+template <int DIM, int HC>
+__global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, float extra,
+                                                         int *gl, int *pool, int pool_lists,
+                                                         unsigned *counter) {
+    __shared__ int s_list[8][32];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    const int K = w.gk;
+    for (long long node = warp; node < n; node += warps) {
+        const float d = w.gd[node];
+        if (signbit(d) || d > t) {
+            if (lane == 0) gl[node] = -1;
+            continue;
+        }
+        const int k = static_cast<int>(node % w.gn[2]);
+        const long long r = node / w.gn[2];
+        const int j = static_cast<int>(r % w.gn[1]);
+        const int i = static_cast<int>(r / w.gn[1]);
+        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+        const float y = w.glo[1] + static_cast<float>(j) * w.gh;
+        const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
+        const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, 1.0f, 0.0f);
+        const float radius = sqrtf(q.best) * (1.0f + 0x1p-16f) + extra;
+        const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list[wib], K);
+        __syncwarp();
+        int idx = -1;
+        if (cnt >= 1 && cnt <= K) {
+            if (lane == 0) idx = static_cast<int>(atomicAdd(counter, 1u));
+            idx = __shfl_sync(kFull, idx, 0);
+            if (idx >= pool_lists) idx = -1;  // cannot happen: the pool holds the band
+        }
+        if (idx >= 0 && lane < K) {
+            pool[static_cast<long long>(idx) * K + lane] = lane < cnt ? s_list[wib][lane] : -1;
+        }
+        if (lane == 0) gl[node] = idx;
+        __syncwarp();
+    }
+}
+}  // namespace
+
+namespace {
+// Contiguous copy of the wide tree's primitive records: slot s at
+// aos[s * (2D: 8, 3D: 16) ...], the fields in their block order.
+__global__ void prim_aos_kernel(WideView w, float *aos) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= w.npad) return;
+    const int nf = w.dim == 2 ? 5 : 16, stride = w.dim == 2 ? 8 : 16;
+    const float *b = w.prim + static_cast<size_t>(s / 32) * nf * 32 + (s % 32);
+    for (int f = 0; f < stride; ++f) aos[static_cast<size_t>(s) * stride + f] = f < nf ? b[f * 32] : 0.0f;
+}
+}  // namespace
+
+size_t prim_aos_bytes(const WideView &w) {
+    return static_cast<size_t>(w.npad) * (w.dim == 2 ? 8 : 16) * sizeof(float);
+}
+
+cudaError_t launch_prim_aos(const WideView &w, float *aos, cudaStream_t stream) {
+    if (w.npad <= 0) return cudaSuccess;
+    prim_aos_kernel<<<static_cast<unsigned>((w.npad + 255) / 256), 256, 0, stream>>>(w, aos);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaStream_t stream) {
+    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const long long blocks = std::min<long long>((n + 255) / 256, 148 * 16);
+    near_band_kernel<<<static_cast<unsigned>(std::max<long long>(blocks, 1)), 256, 0, stream>>>(
+        w.gd, n, t, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
+                              int pool_lists, unsigned *counter, int sms, cudaStream_t stream) {
+    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
+    return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
+        constexpr int HC = decltype(h)::value;
+        if (w.dim == 2) {
+            near_lists_kernel<2, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+                w, t, extra, gl, pool, pool_lists, counter);
+        } else {
+            near_lists_kernel<3, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+                w, t, extra, gl, pool, pool_lists, counter);
+        }
+        return cudaGetLastError();
+    });
+}
+
 size_t lattice_skip_bytes(const WideView &w) {
     const size_t nodes = static_cast<size_t>(w.gn[0]) * w.gn[1] * w.gn[2];
     const size_t rows = static_cast<size_t>(w.gn[1]) * w.gn[2];
@@ -837,7 +965,7 @@ cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin
         if (e != cudaSuccess) return e;
         const unsigned pb = static_cast<unsigned>((s.n_prims + 127) / 128);
         if (w.dim == 2) {
-            row_crossings2_kernel<<<pb, 128, 0, stream>>>(s, w, tol, count, cross);
+            row_crossings2_kernel<<<pb, 128, 0, stream>>>(s, w, count, cross);
         } else {
             row_crossings3_kernel<<<pb, 128, 0, stream>>>(s, w, tol, count, cross);
         }
@@ -931,6 +1059,7 @@ FastArgs make_fast_args(const SceneView &s, const WideView &w, const PointSet &p
     a.shrink = static_cast<float>(1.0 - tau);
     a.shell2 = static_cast<float>(shell * shell);
     a.exact2 = static_cast<float>(shell * shell / ((1.0 - tau) * (1.0 - tau)));
+    a.list_t = w.gl != nullptr ? near_list_threshold(w, epsilon, shell_delta) : -1.0f;
     a.location = location;
     a.start = start;
     a.partials = partials;

@@ -208,17 +208,30 @@ struct WideBuilder {
 // direction (cyclic Jacobi eigen-decomposition of the covariance, rotations
 // from their tangents), offset n.mean and half-thickness max |n.v - offset|.
 // Any unit normal gives a valid slab; the thickness is measured for it.
-static void slab_of(const std::vector<double> &pts, int dim, double *n, double &c, double &h) {
+// The sums run in two levels: over consecutive chunks of `chunk` points
+// (a node's child subtrees), each from zero, then over the chunk sums in
+// order; the device build sums the chunks in parallel in the same order.
+static void slab_of(const std::vector<double> &pts, int dim, size_t chunk, double *n, double &c,
+                    double &h) {
     const size_t m = pts.size() / dim;
     double mean[3] = {0, 0, 0};
-    for (size_t i = 0; i < m; ++i)
-        for (int k = 0; k < dim; ++k) mean[k] += pts[i * dim + k];
+    for (size_t c0 = 0; c0 < m; c0 += chunk) {
+        double part[3] = {0, 0, 0};
+        for (size_t i = c0; i < std::min(m, c0 + chunk); ++i)
+            for (int k = 0; k < dim; ++k) part[k] += pts[i * dim + k];
+        for (int k = 0; k < dim; ++k) mean[k] += part[k];
+    }
     for (int k = 0; k < dim; ++k) mean[k] /= static_cast<double>(m);
     double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (size_t i = 0; i < m; ++i)
+    for (size_t c0 = 0; c0 < m; c0 += chunk) {
+        double part[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (size_t i = c0; i < std::min(m, c0 + chunk); ++i)
+            for (int a = 0; a < dim; ++a)
+                for (int b = 0; b < dim; ++b)
+                    part[a][b] += (pts[i * dim + a] - mean[a]) * (pts[i * dim + b] - mean[b]);
         for (int a = 0; a < dim; ++a)
-            for (int b = 0; b < dim; ++b)
-                A[a][b] += (pts[i * dim + a] - mean[a]) * (pts[i * dim + b] - mean[b]);
+            for (int b = 0; b < dim; ++b) A[a][b] += part[a][b];
+    }
     double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int sweep = 0; sweep < 32; ++sweep) {
         double off = 0.0;
@@ -365,7 +378,7 @@ static void build_wide(HostScene &sc, std::vector<Item> items, int dim) {
                 }
             }
             double nrm[3] = {0, 0, 0}, c = 0.0, th = 0.0;
-            slab_of(pts, dim, nrm, c, th);
+            slab_of(pts, dim, static_cast<size_t>(span_h / 32) * dim, nrm, c, th);
             float nf[3];
             for (int k = 0; k < dim; ++k) nf[k] = static_cast<float>(nrm[k]);
             const float cf = static_cast<float>(c);

@@ -403,40 +403,67 @@ __global__ void wbox_fill_kernel(int dim, float *wbox, int total) {
 }
 
 // Box and slab of every height-h node (build_wide's node loop, slab_of):
-// one thread per node, the node's vertices in wide-slot order.
-__global__ void wide_node_kernel(int dim, int h, long long cnt, long long span, int n,
+// one warp per node.  Lane c sums the points of the node's child c (its
+// `chunk` consecutive points, in wide-slot and vertex order) from zero; lane
+// 0 adds the 32 partial sums in child order, as slab_of does, and fits the
+// slab; the thickness is a maximum, reduced over the lanes.
+__global__ void wide_node_kernel(int dim, long long cnt, long long span, int n,
                                  const double *__restrict__ lv, const int *__restrict__ witem,
                                  const double *__restrict__ verts,
                                  const int *__restrict__ prims, int off, double widen,
                                  float *wbox) {
-    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= cnt) return;
+    constexpr unsigned kAll = 0xffffffffu;
+    const long long i = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= cnt) return;  // whole warps leave together
     const int nc = 2 * dim, nbox = nc + dim + 2;
     float *blk = wbox + off + (i / 32) * nbox * 32;
-    const int lane = static_cast<int>(i % 32);
-    for (int k = 0; k < nc; ++k) {
-        const double v = lv[i * nc + k];
-        blk[k * 32 + lane] = k < dim ? round_down(v - widen) : round_up(v + widen);
+    const int slot_lane = static_cast<int>(i % 32);
+    if (lane == 0) {
+        for (int k = 0; k < nc; ++k) {
+            const double v = lv[i * nc + k];
+            blk[k * 32 + slot_lane] = k < dim ? round_down(v - widen) : round_up(v + widen);
+        }
     }
     const long long s0 = i * span, s1 = min(static_cast<long long>(n), (i + 1) * span);
+    const long long m = (s1 - s0) * dim;
+    const long long chunk = (span / 32) * dim;
+    const long long q0 = lane * chunk, q1 = min(m, q0 + chunk);
     auto point = [&](long long q, int k) {
-        // q-th vertex of the node: slot s0 + q / dim, vertex q % dim
         const long long sl = s0 + q / dim;
         const int v = prims[static_cast<size_t>(dim) * witem[sl] + (q % dim)];
         return verts[static_cast<size_t>(dim) * v + k];
     };
-    const long long m = (s1 - s0) * dim;
+    // mean: chunk sums, then their sum in chunk order
+    double part[3] = {0, 0, 0};
+    for (long long q = q0; q < q1; ++q)
+        for (int k = 0; k < dim; ++k) part[k] += point(q, k);
     double mean[3] = {0, 0, 0};
-    for (long long q = 0; q < m; ++q)
-        for (int k = 0; k < dim; ++k) mean[k] += point(q, k);
-    for (int k = 0; k < dim; ++k) mean[k] /= static_cast<double>(m);
-    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (long long q = 0; q < m; ++q) {
-        double p[3];
-        for (int k = 0; k < dim; ++k) p[k] = point(q, k);
-        for (int a = 0; a < dim; ++a)
-            for (int b = 0; b < dim; ++b) A[a][b] += (p[a] - mean[a]) * (p[b] - mean[b]);
+    for (int c = 0; c < 32; ++c) {
+        for (int k = 0; k < dim; ++k) {
+            const double v = __shfl_sync(kAll, part[k], c);
+            if (static_cast<long long>(c) * chunk < m) mean[k] += v;
+        }
     }
+    for (int k = 0; k < dim; ++k) mean[k] /= static_cast<double>(m);
+    // covariance: the same two levels
+    double pa[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (long long q = q0; q < q1; ++q) {
+        double pt[3];
+        for (int k = 0; k < dim; ++k) pt[k] = point(q, k);
+        for (int a = 0; a < dim; ++a)
+            for (int b = 0; b < dim; ++b) pa[a][b] += (pt[a] - mean[a]) * (pt[b] - mean[b]);
+    }
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int c = 0; c < 32; ++c) {
+        for (int a = 0; a < dim; ++a) {
+            for (int b = 0; b < dim; ++b) {
+                const double v = __shfl_sync(kAll, pa[a][b], c);
+                if (static_cast<long long>(c) * chunk < m) A[a][b] += v;
+            }
+        }
+    }
+    // every lane runs the same Jacobi sweeps on the same matrix
     double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int sweep = 0; sweep < 32; ++sweep) {
         double offd = 0.0;
@@ -486,14 +513,20 @@ __global__ void wide_node_kernel(int dim, int h, long long cnt, long long span, 
     for (int k = 0; k < dim; ++k) nf[k] = static_cast<float>(nrm[k]);
     const float cf = static_cast<float>(c);
     double t32 = 0.0;
-    for (long long q = 0; q < m; ++q) {
+    for (long long q = q0; q < q1; ++q) {
         double t = -static_cast<double>(cf);
         for (int k = 0; k < dim; ++k) t += static_cast<double>(nf[k]) * point(q, k);
         t32 = t32 < fabs(t) ? fabs(t) : t32;
     }
-    for (int k = 0; k < dim; ++k) blk[(nc + k) * 32 + lane] = nf[k];
-    blk[(nc + dim) * 32 + lane] = cf;
-    blk[(nc + dim + 1) * 32 + lane] = round_up(t32 + 4.0 * widen);
+    for (int o = 16; o > 0; o >>= 1) {
+        const double other = __shfl_xor_sync(kAll, t32, o);
+        t32 = t32 < other ? other : t32;
+    }
+    if (lane == 0) {
+        for (int k = 0; k < dim; ++k) blk[(nc + k) * 32 + slot_lane] = nf[k];
+        blk[(nc + dim) * 32 + slot_lane] = cf;
+        blk[(nc + dim + 1) * 32 + slot_lane] = round_up(t32 + 4.0 * widen);
+    }
 }
 
 // Primitive blocks of the wide tree from the binary slots' FP32 records.
@@ -834,9 +867,8 @@ cudaError_t SceneDevice::build_on_device(const HostScene &m, cudaStream_t stream
         long long span = 1;
         for (int h = 1; h < H; ++h) {
             span *= 32;
-            wide_node_kernel<<<blocks_for(cnt[h], 64), 64, 0, stream>>>(
-                dim, h, cnt[h], span, n, lvh[h], witem, d_verts, d_prims, m.w_off[h], widen,
-                wbox);
+            wide_node_kernel<<<blocks_for(cnt[h] * 32, 128), 128, 0, stream>>>(
+                dim, cnt[h], span, n, lvh[h], witem, d_verts, d_prims, m.w_off[h], widen, wbox);
         }
         wprim_kernel<<<blocks_for(m.w_npad), 256, 0, stream>>>(dim, n, m.w_npad, wide2bin, rec32,
                                                                inv32, wprim);
