@@ -192,7 +192,8 @@ __device__ __forceinline__ WideResult lane_nearest(const WideView &w, float px, 
 
 // Closest primitive among a near-boundary candidate list (at most k wide
 // slots, -1 past the end), found by this lane alone; the first minimum in
-// list order wins.
+// list order wins.  Records come from the contiguous copy (w.aos), or from
+// the cluster blocks when a kernel staged those in shared memory (aos null).
 template <int DIM>
 __device__ __forceinline__ WideResult list_nearest(const WideView &w, const int *list, int k,
                                                    float px, float py, float pz) {
@@ -202,7 +203,11 @@ __device__ __forceinline__ WideResult list_nearest(const WideView &w, const int 
         const int s = __ldg(list + q);
         if (s < 0) break;
         float d2;
-        if (DIM == 2) {
+        if (w.aos == nullptr) {
+            // the cluster blocks (staged in shared memory by the caller)
+            constexpr int NF = DIM == 2 ? 5 : 16;
+            d2 = prim_dist<DIM>(w.prim + (s >> 5) * (NF * 32) + (s & 31), px, py, pz);
+        } else if (DIM == 2) {
             const float4 a = __ldg(w.aos + 2 * s);
             const float inv = __ldg(reinterpret_cast<const float *>(w.aos + 2 * s + 1));
             const float wx = px - a.x, wy = py - a.y;

@@ -303,7 +303,11 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) walk_fast_kernel(FastArgs a, 
         }
         __syncthreads();
         wv.box = sm;
-        if (a.stage_prim) wv.prim = sm + a.stage_box;
+        if (a.stage_prim) {
+            // staged primitives: the list scans read them here, not the copy
+            wv.prim = sm + a.stage_box;
+            wv.aos = nullptr;
+        }
     }
     const int lane = threadIdx.x & 31;
 
