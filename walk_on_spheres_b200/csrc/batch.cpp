@@ -129,7 +129,7 @@ int wos_batch::prepare() {
     std::stable_sort(todo.begin(), todo.end(), [](const BatchMesh *a, const BatchMesh *b) {
         return a->prims.size() > b->prims.size();
     });
-    if (device_tree_build()) {
+    if (device_tree_build(true)) {
         // every tree on the device, one mesh after another on the stream,
         // each followed by its lattice; the host only checks the meshes
         cudaSetDevice(ctx->device);

@@ -327,9 +327,11 @@ void SceneDevice::release() {
     slot_verts = nullptr;
 }
 
-bool wosb::device_tree_build() {
+bool wosb::device_tree_build(bool batch) {
     const char *e = std::getenv("WOS_TREE_BUILD");
-    return !(e && std::string(e) == "host");
+    if (e && std::string(e) == "host") return false;
+    if (e && std::string(e) == "device") return true;
+    return !batch;
 }
 
 int wos_context::upload_scene() {
@@ -352,7 +354,7 @@ extern "C" int wos_set_mesh(wos_context *ctx, int dim, const double *verts, int 
     HostScene sc;
     // the device build needs only the checked mesh and its metadata
     const std::string err =
-        device_tree_build()
+        device_tree_build(false)
             ? scene_meta(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, sc)
             : build_scene(dim, verts, n_verts, prims, n_prims, boundary_ids, leaf_size, sc);
     if (!err.empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + err);

@@ -65,9 +65,11 @@ struct SceneDevice {
 
 double effective_epsilon(const wos_params &p);
 
-// Where trees are built: on the device (default) or, with
-// WOS_TREE_BUILD=host, on the host threads; both give the same arrays.
-bool device_tree_build();
+// Where trees are built; both builders give the same arrays.  A single mesh
+// (wos_set_mesh) is built on the device unless WOS_TREE_BUILD=host; a
+// batch's meshes on the host threads, in parallel with the device's lattice
+// builds, unless WOS_TREE_BUILD=device.
+bool device_tree_build(bool batch);
 
 // Argument checks shared by the grid entry points: an empty string when
 // `p` (against the context's mesh) or the grid is acceptable, else the
