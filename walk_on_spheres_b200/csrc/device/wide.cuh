@@ -307,16 +307,13 @@ inline auto with_height_class(int hc, F &&f) {
 
 // Closest primitive to (px, py, pz); all 32 lanes of the warp must call this
 // with the same point and receive the same result.  HC: the height class the
-// caller guarantees (height_class(w.H) == HC), or kHeightAny.  limit0: an
-// upper bound of the squared distance, if the caller knows one (children
-// whose lower bound reaches it are not visited); slot -1 if it was too small.
+// caller guarantees (height_class(w.H) == HC), or kHeightAny.
 template <int DIM, int HC = kHeightAny>
 __device__ __forceinline__ WideResult wide_nearest(const WideView &w, float px, float py,
-                                                   float pz, float keep, float exact2,
-                                                   float limit0 = INFINITY) {
+                                                   float pz, float keep, float exact2) {
     constexpr unsigned kAll = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
-    float best = INFINITY, limit = limit0;
+    float best = INFINITY, limit = INFINITY;
     int slot = -1;
     auto leaf = [&](int cluster) {
         const float d2 = wide_prim_dist<DIM>(w, cluster, px, py, pz);

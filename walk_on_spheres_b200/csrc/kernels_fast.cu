@@ -655,57 +655,37 @@ __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin
     const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
     constexpr int kNeighbours = DIM == 2 ? 9 : 27;
-    // each warp takes runs of kRun consecutive nodes (neighbours along the
-    // last axis): a node's query starts from the upper bound
-    // d(previous node) + |p - previous| of its distance, so it visits only
-    // children that can hold the nearest primitive
-    constexpr int kRun = 8;
-    for (long long run = warp; run * kRun < n; run += warps) {
-        float prev = INFINITY;  // sqrt(best) at the last queried node
-        float qx = 0.0f, qy = 0.0f, qz = 0.0f;
-        for (int u = 0; u < kRun; ++u) {
-            const long long t = run * kRun + u;
-            if (t >= n) break;
-            const int k = static_cast<int>(t % w.gn[2]);
-            const long long r = t / w.gn[2];
-            const int j = static_cast<int>(r % w.gn[1]);
-            const int i = static_cast<int>(r / w.gn[1]);
-            if (outside != nullptr) {
-                // a node whose own and neighbours' centres are all outside the
-                // mesh stores 0 (a valid lower bound) without a query: no walk
-                // inside the domain samples it for a useful bound
-                bool out_n = true;
-                if (lane < kNeighbours) {
-                    const int ni = i + lane % 3 - 1, nj = j + (lane / 3) % 3 - 1;
-                    const int nk = DIM == 3 ? k + lane / 9 - 1 : 0;
-                    if (ni >= 0 && ni < w.gn[0] && nj >= 0 && nj < w.gn[1] && nk >= 0 &&
-                        nk < w.gn[2]) {
-                        out_n = outside[(static_cast<long long>(ni) * w.gn[1] + nj) * w.gn[2] + nk] != 0;
-                    }
-                }
-                if (__all_sync(kFull, out_n)) {
-                    // -0.0: a valid bound that marks the node as skipped
-                    if (lane == 0) out[t] = -0.0f;
-                    continue;
+    for (long long t = warp; t < n; t += warps) {
+        const int k = static_cast<int>(t % w.gn[2]);
+        const long long r = t / w.gn[2];
+        const int j = static_cast<int>(r % w.gn[1]);
+        const int i = static_cast<int>(r / w.gn[1]);
+        if (outside != nullptr) {
+            // a node whose own and neighbours' centres are all outside the
+            // mesh stores 0 (a valid lower bound) without a query: no walk
+            // inside the domain samples it for a useful bound
+            bool out_n = true;
+            if (lane < kNeighbours) {
+                const int ni = i + lane % 3 - 1, nj = j + (lane / 3) % 3 - 1;
+                const int nk = DIM == 3 ? k + lane / 9 - 1 : 0;
+                if (ni >= 0 && ni < w.gn[0] && nj >= 0 && nj < w.gn[1] && nk >= 0 &&
+                    nk < w.gn[2]) {
+                    out_n = outside[(static_cast<long long>(ni) * w.gn[1] + nj) * w.gn[2] + nk] != 0;
                 }
             }
-            const float x = w.glo[0] + static_cast<float>(i) * w.gh;
-            const float y = w.glo[1] + static_cast<float>(j) * w.gh;
-            const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-            // d(p) <= d(prev) <= sqrt(best at prev) plus the step; 2^-10 covers
-            // the FP32 rounding of both
-            const float dx = x - qx, dy = y - qy, dz = z - qz;
-            const float up = (prev + sqrtf(dx * dx + dy * dy + dz * dz)) * (1.0f + 0x1p-10f);
-            WideResult q = wide_nearest<DIM, HC>(w, x, y, z, kShrink * kShrink, 0.0f, up * up);
-            if (q.slot < 0) q = wide_nearest<DIM, HC>(w, x, y, z, kShrink * kShrink, 0.0f);
-            prev = sqrtf(q.best);
-            qx = x;
-            qy = y;
-            qz = z;
-            if (lane == 0) {
-                const float d = (prev * kShrink - margin) * (1.0f - 0x1p-20f);
-                out[t] = d > 0.0f ? d : 0.0f;
+            if (__all_sync(kFull, out_n)) {
+                // -0.0: a valid bound that marks the node as skipped
+                if (lane == 0) out[t] = -0.0f;
+                continue;
             }
+        }
+        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+        const float y = w.glo[1] + static_cast<float>(j) * w.gh;
+        const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
+        const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, kShrink * kShrink, 0.0f);
+        if (lane == 0) {
+            const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
+            out[t] = d > 0.0f ? d : 0.0f;
         }
     }
 }
@@ -998,9 +978,7 @@ cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin
             w, tol, count, cross, outside);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    // one warp per run of 8 nodes
-    const long long blocks =
-        std::min<long long>((n + 63) / 64, static_cast<long long>(sms) * 8);
+    const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
     // compiled per traversal class, like the walk kernels
     return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
         constexpr int HC = decltype(h)::value;
