@@ -96,10 +96,10 @@ REF_STRIDE = 128
 # distance lattice read once and the fields written: the same at any walk
 # count), and the L2 peak the capture implies (lts__t_bytes.sum.per_second
 # over lts__t_sectors.sum.pct_of_peak_sustained_elapsed).
-NCU_PER_STEP = {"uniform": {"issued": 4682003701 / 148762432, "l2_bytes": 10.170560e9 / 148762432},
-                "green": {"issued": 4706918360 / 148738671, "l2_bytes": 10.170313e9 / 148738671}}
+NCU_PER_STEP = {"uniform": {"issued": 3257663940 / 148740981, "l2_bytes": 7.581465e9 / 148740981},
+                "green": {"issued": 3218209969 / 148751403, "l2_bytes": 7.580572e9 / 148751403}}
 NCU_DRAM_BYTES_PER_LAUNCH = 22.2e6
-NCU_L2_PEAK_GBS = 1864.443 / 0.05374150
+NCU_L2_PEAK_GBS = 1990.496 / 0.05747237
 ISSUE_SLOTS_PER_SM_CYCLE = 4   # one warp instruction per SM sub-partition per cycle
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
 # 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in

@@ -198,6 +198,9 @@ cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
         return e;
     }
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    // list indices are packed above a 6-bit length (int entries); the
+    // lattices hold at most 2^24 nodes, so this never binds
+    band = std::min(band, (1u << 25) - 1u);
     WideView w = wide;
     w.gk = near_list_capacity(w.dim);
     if (const char *env = std::getenv("WOS_NEAR_CAPACITY")) {

@@ -50,12 +50,17 @@ __device__ __forceinline__ T dist(V3<T> a, V3<T> b) {
 }
 
 // Angles: the exact path forms theta in double and calls cos/sin like the
-// reference; the fast path uses sincospi on 2u (no range reduction).
+// reference.  FAST_FP64 uses sincospi on 2u.  FAST_FP32 takes the hardware
+// sine/cosine of 2 pi u - pi, an angle in [-pi, pi] where their absolute error
+// is documented as at most 2^-21.41 (a uniform angle turned by pi is still
+// uniform).  That moves a step point by under 4e-7 R, far inside the
+// 2^-10 relative margin of every FP32 radius; inside the epsilon shell the
+// walk re-projects in FP64 anyway.
 template <typename T>
 __device__ __forceinline__ void sincos_2pi(T u, T &s, T &c);
 template <>
 __device__ __forceinline__ void sincos_2pi<float>(float u, float &s, float &c) {
-    sincospif(2.0f * u, &s, &c);
+    __sincosf(fmaf(u, 6.28318531f, -3.14159265f), &s, &c);
 }
 template <>
 __device__ __forceinline__ void sincos_2pi<double>(double u, double &s, double &c) {

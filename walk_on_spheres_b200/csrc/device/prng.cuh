@@ -93,27 +93,56 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
     return ctr;
 }
 
-// One walk's stream: counter (block, walk, tag, 0) under the point's key.
+// One walk's stream under the point's key: counter (block, walk, tag, step).
+// begin_step(s) starts step s at a fresh block, so every lane of a warp runs
+// the Philox rounds at that one point of the step instead of wherever its
+// four-value buffer happens to run dry; draws past the first four of a step
+// take the step's next blocks.  Values left over at the end of a step are
+// dropped.
 struct PhiloxStream {
     uint2 key;
     uint32_t walk;
     uint32_t block;
+    uint32_t base;  // first block of every step (the tag's range)
+    uint32_t step;
     uint32_t b0, b1, b2, b3;
     int left;
 
-    __device__ __forceinline__ PhiloxStream(uint64_t point_seed_value, uint32_t walk_index,
-                                            uint32_t tag = 0) {
+    // The key of a point's streams (the same for all of its walks).
+    static __device__ __forceinline__ uint2 key_of(uint64_t point_seed_value) {
         const uint64_t k = splitmix64(point_seed_value ^ kFastStream);
-        key = make_uint2(static_cast<uint32_t>(k), static_cast<uint32_t>(k >> 32));
+        return make_uint2(static_cast<uint32_t>(k), static_cast<uint32_t>(k >> 32));
+    }
+
+    __device__ __forceinline__ PhiloxStream(uint64_t point_seed_value, uint32_t walk_index,
+                                            uint32_t tag = 0)
+        : PhiloxStream(key_of(point_seed_value), walk_index, tag) {}
+
+    __device__ __forceinline__ PhiloxStream(uint2 point_key, uint32_t walk_index,
+                                            uint32_t tag = 0) {
+        key = point_key;
         walk = walk_index;
         block = tag << 24;  // disjoint block ranges per tag (2^24 blocks each)
+        base = block;
+        step = 0;
         left = 0;
         b0 = b1 = b2 = b3 = 0;
     }
 
+    __device__ __forceinline__ void begin_step(uint32_t s) {
+        step = s;
+        block = base;
+        const uint4 r = philox4x32_10(make_uint4(block++, walk, 0x5A17u, step), key);
+        b0 = r.x;
+        b1 = r.y;
+        b2 = r.z;
+        b3 = r.w;
+        left = 4;
+    }
+
     __device__ __forceinline__ uint32_t next_u32() {
         if (left == 0) {
-            const uint4 r = philox4x32_10(make_uint4(block++, walk, 0x5A17u, 0u), key);
+            const uint4 r = philox4x32_10(make_uint4(block++, walk, 0x5A17u, step), key);
             b0 = r.x;
             b1 = r.y;
             b2 = r.z;

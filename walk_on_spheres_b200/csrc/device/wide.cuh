@@ -58,8 +58,8 @@ struct WideView {
     // of the upper bound D + r of the true distance
     float gratio;
     // Near-boundary candidate lists (null when absent): gl[node] is -1 or
-    // the index of the node's list, gk wide slots at gpool + gl[node] * gk
-    // (-1 past its end).  The list holds every primitive within
+    // (list index << 6) | length, the list's wide slots at
+    // gpool + index * gk (-1 past its length).  The list holds every primitive within
     // d(node) + 2 r_max of the node (r_max the largest distance from a point
     // to its nearest node), so it holds the nearest primitive of every point
     // whose nearest node this is.
@@ -190,10 +190,39 @@ __device__ __forceinline__ WideResult lane_nearest(const WideView &w, float px, 
     return WideResult{best, slot};
 }
 
-// Closest primitive among a near-boundary candidate list (at most k wide
-// slots, -1 past the end), found by this lane alone; the first minimum in
-// list order wins.  Records come from the contiguous copy (w.aos), or from
-// the cluster blocks when a kernel staged those in shared memory (aos null).
+// Squared FP32 distance from p to the primitive in wide slot s, read from
+// the contiguous records (w.aos), or from the cluster blocks when a kernel
+// staged those in shared memory (aos null).
+template <int DIM>
+__device__ __forceinline__ float slot_dist(const WideView &w, int s, float px, float py,
+                                           float pz) {
+    if (w.aos == nullptr) {
+        constexpr int NF = DIM == 2 ? 5 : 16;
+        return prim_dist<DIM>(w.prim + (s >> 5) * (NF * 32) + (s & 31), px, py, pz);
+    }
+    if (DIM == 2) {
+        const float4 a = __ldg(w.aos + 2 * s);
+        const float inv = __ldg(reinterpret_cast<const float *>(w.aos + 2 * s + 1));
+        const float wx = px - a.x, wy = py - a.y;
+        const float t = fminf(fmaxf((wx * a.z + wy * a.w) * inv, 0.0f), 1.0f);
+        const float dx = wx - t * a.z, dy = wy - t * a.w;
+        return dx * dx + dy * dy;
+    }
+    float4 rec[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) rec[f] = __ldg(w.aos + 4 * s + f);
+    return eberly32(px, py, pz, rec);
+}
+
+// A node's packed list entry gl[node] = (list index << 6) | length, or -1.
+__device__ __forceinline__ const int *list_of(const WideView &w, int packed) {
+    return w.gpool + static_cast<long long>(packed >> 6) * w.gk;
+}
+__device__ __forceinline__ int list_length(int packed) { return packed & 63; }
+
+// Closest primitive among a near-boundary candidate list of k wide slots,
+// found by this lane alone; the first minimum in list order (ascending
+// slots) wins.
 template <int DIM>
 __device__ __forceinline__ WideResult list_nearest(const WideView &w, const int *list, int k,
                                                    float px, float py, float pz) {
@@ -201,31 +230,77 @@ __device__ __forceinline__ WideResult list_nearest(const WideView &w, const int 
     int slot = -1;
     for (int q = 0; q < k; ++q) {
         const int s = __ldg(list + q);
-        if (s < 0) break;
-        float d2;
-        if (w.aos == nullptr) {
-            // the cluster blocks (staged in shared memory by the caller)
-            constexpr int NF = DIM == 2 ? 5 : 16;
-            d2 = prim_dist<DIM>(w.prim + (s >> 5) * (NF * 32) + (s & 31), px, py, pz);
-        } else if (DIM == 2) {
-            const float4 a = __ldg(w.aos + 2 * s);
-            const float inv = __ldg(reinterpret_cast<const float *>(w.aos + 2 * s + 1));
-            const float wx = px - a.x, wy = py - a.y;
-            const float t = fminf(fmaxf((wx * a.z + wy * a.w) * inv, 0.0f), 1.0f);
-            const float dx = wx - t * a.z, dy = wy - t * a.w;
-            d2 = dx * dx + dy * dy;
-        } else {
-            float4 rec[4];
-#pragma unroll
-            for (int f = 0; f < 4; ++f) rec[f] = __ldg(w.aos + 4 * s + f);
-            d2 = eberly32(px, py, pz, rec);
-        }
+        const float d2 = slot_dist<DIM>(w, s, px, py, pz);
         if (d2 < best) {
             best = d2;
             slot = s;
         }
     }
     return WideResult{best, slot};
+}
+
+// list_nearest's answer for every lane with `want` (`packed` its node's list
+// entry), computed by the whole warp, which must call it converged.  The
+// (lane, candidate) pairs of all wanting lanes are laid out 32 at a time
+// across the lanes; each lane measures one pair; a segmented minimum over
+// (distance bits, slot) keys hands each list's winner to its lane, so ties
+// go to the lower slot as in list_nearest.  A lane alone would scan its whole
+// list while the others wait.
+template <int DIM>
+__device__ __forceinline__ WideResult warp_list_nearest(const WideView &w, bool want, int packed,
+                                                        float px, float py, float pz) {
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr unsigned long long kNone = ~0ull;
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int k = want ? list_length(packed) : 0;
+    int inc = k;  // inclusive prefix sum of the lengths
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kAll, inc, o);
+        if (lane >= o) inc += t;
+    }
+    const int total = __shfl_sync(kAll, inc, 31);
+    const int off = inc - k;  // this lane's first pair
+    const int first = want ? (packed >> 6) * w.gk : 0;  // < 2^30: index < 2^24, gk <= 32
+    unsigned long long best = kNone;
+    for (int c = 0; c < total; c += 32) {
+        const int g = c + lane;  // the pair this lane measures
+        // its owner: the last lane whose first pair is at or before g
+        // (offsets never decrease along the lanes; j + step stays <= 31)
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            if (__shfl_sync(kAll, off, j + step) <= g) j += step;
+        }
+        const int q = g - __shfl_sync(kAll, off, j);
+        const int list = __shfl_sync(kAll, first, j);
+        const float qx = __shfl_sync(kAll, px, j);
+        const float qy = __shfl_sync(kAll, py, j);
+        const float qz = DIM == 3 ? __shfl_sync(kAll, pz, j) : 0.0f;
+        unsigned long long key = kNone;
+        if (g < total) {
+            const int s = __ldg(w.gpool + list + q);
+            const float d2 = slot_dist<DIM>(w, s, qx, qy, qz);
+            if (d2 < INFINITY) {
+                key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                      static_cast<unsigned>(s);
+            }
+        }
+        // minimum over the rest of this lane's run (one owner's lanes are
+        // contiguous; lanes past the total carry no key)
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long other = __shfl_down_sync(kAll, key, o);
+            const int jo = __shfl_down_sync(kAll, j, o);
+            if (lane + o < 32 && jo == j && other < key) key = other;
+        }
+        // each owner reads the first lane of its run in this chunk
+        const unsigned long long run = __shfl_sync(kAll, key, min(max(off - c, 0), 31));
+        if (k > 0 && off < c + 32 && off + k > c && run < best) best = run;
+    }
+    if (best == kNone) return WideResult{INFINITY, -1};
+    return WideResult{__uint_as_float(static_cast<unsigned>(best >> 32)),
+                      static_cast<int>(static_cast<unsigned>(best))};
 }
 
 // Every primitive within squared FP32 distance r2 of (px, py, pz), found by

@@ -259,8 +259,8 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
         const int w0 = c * a.chunk;
         const int w1 = min(a.n_walks, w0 + a.chunk);
 
-        int n_acc = 0, steps_acc = 0;
-        double mean_acc = 0.0, m2_acc = 0.0;
+        int steps_acc = 0;
+        ShiftedSums acc;
         // per-lane sums and sums of squares of the derivatives, in shared
         // memory (touched once per finished walk) to keep registers for the walk
         if (adj) {
@@ -282,12 +282,14 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
         int slot = -1;                    // FP32: wide slot of the last query
         int slot64 = -1;                  // FP64: binary slot of the last query
         V3<double> np64{0.0, 0.0, 0.0};
-        FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
+        const uint2 pkey = PhiloxStream::key_of(pseed);
+        FastRng<T> rng(pkey, static_cast<uint32_t>(walk));
 
         while (__any_sync(kFull, active)) {
             bool done = false;
             bool need_query = false;
             bool listed = false;  // answered from a near-boundary list
+            int packed = -1;      // 3D: the list the warp scans for this lane
             double value = 0.0;
             if (active) {
                 bool stop = false;
@@ -310,13 +312,13 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                         stop = true;
                     } else {
                         bslot = wv.wide2bin[slot];
-                        const double d64 = reproject64<DIM>(
+                        const double d2 = reproject64_sq<DIM>(
                             a.s, bslot, static_cast<double>(p.x), static_cast<double>(p.y),
                             static_cast<double>(p.z), np, bid);
-                        if (d64 <= eps) {
+                        if (d2 <= eps * eps) {
                             stop = true;
                         } else {
-                            R = static_cast<T>(d64);
+                            R = static_cast<T>(sqrt(d2));
                         }
                     }
                 }
@@ -341,6 +343,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                     value = sample + (bslot >= 0 ? boundary_data<DIM>(a, bslot, np, cgrad) : 0.0);
                     done = true;
                 } else {
+                    rng.begin_step(steps);
                     sample += heat_source<DIM, T>(a, p, R, rng, adj, j);
                     p = sphere_step<DIM, false, T>(p, R, rng);
                     ++steps;
@@ -357,17 +360,21 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                                 R = gb;
                                 need_query = false;
                             } else if (ls.d <= a.list_t) {
-                                // near the boundary: this lane's own query over
-                                // the node's candidate list, when it has one
-                                const int li = __ldg(wv.gl + ls.node);
-                                if (li >= 0) {
-                                    const WideResult q = list_nearest<DIM>(
-                                        wv, wv.gpool + static_cast<long long>(li) * wv.gk, wv.gk,
-                                        static_cast<float>(p.x), static_cast<float>(p.y),
-                                        static_cast<float>(p.z));
-                                    const float r = sqrtf(q.best);
-                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
-                                    slot = q.slot;
+                                // near the boundary: a query over the node's
+                                // candidate list, when it has one (2D: this
+                                // lane scans it; 3D: the warp, below)
+                                const int v = __ldg(wv.gl + ls.node);
+                                if (v >= 0) {
+                                    if constexpr (DIM == 2) {
+                                        const WideResult q = list_nearest<DIM>(
+                                            wv, list_of(wv, v), list_length(v),
+                                            static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
+                                        const float r = sqrtf(q.best);
+                                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                        slot = q.slot;
+                                    } else {
+                                        packed = v;
+                                    }
                                     need_query = false;
                                     listed = true;
                                 }
@@ -380,6 +387,19 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                         R = static_cast<T>(sqrt(q.best));
                         np64 = V3<double>{q.x, q.y, q.z};
                         slot64 = q.slot;
+                    }
+                }
+            }
+            if constexpr (kF32 && DIM == 3) {
+                const bool want = packed >= 0;
+                if (__any_sync(kFull, want)) {
+                    const WideResult q = warp_list_nearest<DIM>(
+                        wv, want, packed, static_cast<float>(p.x), static_cast<float>(p.y),
+                        static_cast<float>(p.z));
+                    if (want) {
+                        const float r = sqrtf(q.best);
+                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                        slot = q.slot;
                     }
                 }
             }
@@ -408,10 +428,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                 }
             }
             if (done) {
-                ++n_acc;
-                const double before = value - mean_acc;
-                mean_acc += before / static_cast<double>(n_acc);
-                m2_acc += before * (value - mean_acc);
+                acc.add(value);
                 steps_acc += steps;
                 if (adj) {
 #pragma unroll
@@ -433,7 +450,7 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
 #pragma unroll
                         for (int k = 0; k < 5; ++k) j[k] = 0.0;
                         steps = 0;
-                        rng = FastRng<T>(pseed, static_cast<uint32_t>(walk));
+                        rng = FastRng<T>(pkey, static_cast<uint32_t>(walk));
                     }
                 }
                 next += __popc(done_mask);
@@ -441,7 +458,9 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
         }
 
         if (__ballot_sync(kFull, bad) && lane == 0) atomicOr(&a.ctr->error_flags, kErrBadState);
-        double n_tot = static_cast<double>(n_acc);
+        double n_tot = static_cast<double>(acc.n);
+        double mean_acc, m2_acc;
+        acc.finish(mean_acc, m2_acc);
         unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

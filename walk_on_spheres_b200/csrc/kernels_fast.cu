@@ -38,6 +38,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const double eps = a.eps;
+    const double eps2 = eps * eps;
 
     double x0, y0, z0;
     uint64_t linear;
@@ -51,8 +52,8 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     const int w1 = min(a.n_walks, w0 + a.chunk);
 
     // per-lane statistics
-    int n_acc = 0, steps_acc = 0;
-    double mean_acc = 0.0, m2_acc = 0.0;
+    int steps_acc = 0;
+    ShiftedSums acc;
     unsigned hits = 0;
     // BVH closest-point queries of this task (warp-uniform; FP32 only: every
     // FP64 step is one).  At most chunk * max_steps < 2^32 (set_chunk).
@@ -71,12 +72,14 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     int slot = -1;                 // FP32: winner of the last query
     V3<double> np64{0.0, 0.0, 0.0};  // FP64: nearest point of the last query
     int bid64 = -1;
-    FastRng<T> rng(pseed, static_cast<uint32_t>(walk));
+    const uint2 pkey = PhiloxStream::key_of(pseed);
+    FastRng<T> rng(pkey, static_cast<uint32_t>(walk));
 
     while (__any_sync(kFull, active)) {
         bool done = false;
         bool need_query = false;
         bool listed = false;  // answered from a near-boundary list
+        int packed = -1;      // 3D: the list the warp scans for this lane
         double value = 0.0;
         if (active) {
             bool stop = false;
@@ -100,14 +103,14 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                     bad = true;
                     stop = true;
                 } else {
-                    const double d64 = reproject64<DIM>(a.s, wv.wide2bin[slot],
-                                                        static_cast<double>(p.x),
-                                                        static_cast<double>(p.y),
-                                                        static_cast<double>(p.z), np, bid);
-                    if (d64 <= eps) {
+                    const double d2 = reproject64_sq<DIM>(a.s, wv.wide2bin[slot],
+                                                          static_cast<double>(p.x),
+                                                          static_cast<double>(p.y),
+                                                          static_cast<double>(p.z), np, bid);
+                    if (d2 <= eps2) {
                         stop = true;
                     } else {
-                        R = static_cast<T>(d64);
+                        R = static_cast<T>(sqrt(d2));
                     }
                 }
             }
@@ -134,6 +137,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                         static_cast<double>(weight) * eq.boundary(np, bid);
                 done = true;
             } else {
+                rng.begin_step(steps);
                 p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
                 ++steps;
                 if constexpr (kF32) {
@@ -150,17 +154,22 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                                 R = gb;
                                 need_query = false;
                             } else if (ls.d <= a.list_t) {
-                                // near the boundary: this lane's own query over
-                                // the node's candidate list, when it has one
-                                const int li = __ldg(wv.gl + ls.node);
-                                if (li >= 0) {
-                                    const WideResult q = list_nearest<DIM>(
-                                        wv, wv.gpool + static_cast<long long>(li) * wv.gk, wv.gk,
-                                        static_cast<float>(p.x), static_cast<float>(p.y),
-                                        static_cast<float>(p.z));
-                                    const float r = sqrtf(q.best);
-                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
-                                    slot = q.slot;
+                                // near the boundary: a query over the node's
+                                // candidate list, when it has one; in 2D (a
+                                // few segments) this lane scans it, in 3D the
+                                // warp scans all such lists together below
+                                const int v = __ldg(wv.gl + ls.node);
+                                if (v >= 0) {
+                                    if constexpr (DIM == 2) {
+                                        const WideResult q = list_nearest<DIM>(
+                                            wv, list_of(wv, v), list_length(v),
+                                            static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
+                                        const float r = sqrtf(q.best);
+                                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                        slot = q.slot;
+                                    } else {
+                                        packed = v;
+                                    }
                                     need_query = false;
                                     listed = true;
                                 }
@@ -189,6 +198,19 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 slot = q.slot;
             }
         } else if constexpr (kF32) {
+            if constexpr (DIM == 3) {
+                const bool want = packed >= 0;
+                if (__any_sync(kFull, want)) {
+                    const WideResult q = warp_list_nearest<DIM>(
+                        wv, want, packed, static_cast<float>(p.x), static_cast<float>(p.y),
+                        static_cast<float>(p.z));
+                    if (want) {
+                        const float r = sqrtf(q.best);
+                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                        slot = q.slot;
+                    }
+                }
+            }
             // the warp resolves every pending closest-point query together
             unsigned pending = __ballot_sync(kFull, need_query);
             queries += __popc(pending) + __popc(__ballot_sync(kFull, listed));
@@ -214,10 +236,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
         }
         if (done) {
             // Welford update of this lane's statistics
-            ++n_acc;
-            const double before = value - mean_acc;
-            mean_acc += before / static_cast<double>(n_acc);
-            m2_acc += before * (value - mean_acc);
+            acc.add(value);
             steps_acc += steps;
         }
         const unsigned done_mask = __ballot_sync(kFull, done);
@@ -231,7 +250,7 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                     sample = T(0);
                     weight = T(1);
                     steps = 0;
-                    rng = FastRng<T>(pseed, static_cast<uint32_t>(walk));
+                    rng = FastRng<T>(pkey, static_cast<uint32_t>(walk));
                 }
             }
             next += __popc(done_mask);
@@ -239,7 +258,9 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     }
 
     // warp merge of the lanes' statistics
-    double n_tot = static_cast<double>(n_acc);
+    double n_tot = static_cast<double>(acc.n);
+    double mean_acc, m2_acc;
+    acc.finish(mean_acc, m2_acc);
     unsigned long long steps_tot = static_cast<unsigned long long>(steps_acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -889,7 +910,8 @@ __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, fl
         if (idx >= 0 && lane < K) {
             pool[static_cast<long long>(idx) * K + lane] = lane < cnt ? s_list[wib][lane] : -1;
         }
-        if (lane == 0) gl[node] = idx;
+        // packed entry: (list index << 6) | length (index < 2^24, length <= 32)
+        if (lane == 0) gl[node] = idx >= 0 ? (idx << 6) | cnt : -1;
         __syncwarp();
     }
 }
