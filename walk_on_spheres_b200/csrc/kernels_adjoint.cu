@@ -286,22 +286,108 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
         FastRng<T> rng(pkey, static_cast<uint32_t>(walk));
 
         while (__any_sync(kFull, active)) {
-            bool done = false;
             bool need_query = false;
             bool listed = false;  // answered from a near-boundary list
             int packed = -1;      // 3D: the list the warp scans for this lane
+            // one step of every walk in flight (none from a start point
+            // inside the shell)
+            if (active && !start_stops) {
+                rng.begin_step(steps);
+                sample += heat_source<DIM, T>(a, p, R, rng, adj, j);
+                p = sphere_step<DIM, false, T>(p, R, rng);
+                ++steps;
+                if constexpr (kF32) {
+                    need_query = true;
+                    // the walk kernels' lattice step: away from the shell a
+                    // lattice lower bound is the radius (forward and replay
+                    // take the same branches, the lattice is fixed)
+                    if (wv.gd != nullptr && steps < a.max_steps) {
+                        const LatticeSample ls =
+                            lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
+                        const float gb = (ls.d - ls.r) * a.shrink;
+                        if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
+                            R = gb;
+                            need_query = false;
+                        } else if (ls.d <= a.list_t) {
+                            // near the boundary: a query over the node's
+                            // candidate list, when it has one (2D: this
+                            // lane scans it; 3D: the warp, below)
+                            const int v = __ldg(wv.gl + ls.node);
+                            if (v >= 0) {
+                                if constexpr (DIM == 2) {
+                                    const WideResult q = list_nearest<DIM>(
+                                        wv, list_of(wv, v), list_length(v),
+                                        static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
+                                    const float r = sqrtf(q.best);
+                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                    slot = q.slot;
+                                } else {
+                                    packed = v;
+                                }
+                                need_query = false;
+                                listed = true;
+                            }
+                        }
+                    }
+                } else {
+                    const Nearest<double> q = nearest64<DIM>(
+                        a.s, static_cast<double>(p.x), static_cast<double>(p.y),
+                        static_cast<double>(p.z), dinf());
+                    R = static_cast<T>(sqrt(q.best));
+                    np64 = V3<double>{q.x, q.y, q.z};
+                    slot64 = q.slot;
+                }
+            }
+            if constexpr (kF32 && DIM == 3) {
+                const bool want = packed >= 0;
+                if (__any_sync(kFull, want)) {
+                    const WideResult q = warp_list_nearest<DIM>(
+                        wv, want, packed, static_cast<float>(p.x), static_cast<float>(p.y),
+                        static_cast<float>(p.z));
+                    if (want) {
+                        const float r = sqrtf(q.best);
+                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                        slot = q.slot;
+                    }
+                }
+            }
+            if constexpr (kF32) {
+                unsigned pending = __ballot_sync(kFull, need_query);
+                queries += __popc(pending) + __popc(__ballot_sync(kFull, listed));
+                float qbest = 0.0f;
+                int qslot = -1;
+                while (pending) {
+                    const int jl = __ffs(pending) - 1;
+                    pending &= pending - 1u;
+                    const float qx = __shfl_sync(kFull, static_cast<float>(p.x), jl);
+                    const float qy = __shfl_sync(kFull, static_cast<float>(p.y), jl);
+                    const float qz =
+                        DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), jl) : 0.0f;
+                    const WideResult r = wide_nearest<DIM, HC>(wv, qx, qy, qz, a.keep, a.exact2);
+                    if (lane == jl) {
+                        qbest = r.best;
+                        qslot = r.slot;
+                    }
+                }
+                if (need_query) {
+                    const float r = sqrtf(qbest);
+                    R = static_cast<T>(qbest > a.shell2 ? r * a.shrink : r);
+                    slot = qslot;
+                }
+            }
+            // walks whose new radius is in the shell, or that reached the
+            // step cap, end in the iteration of their last step
+            bool done = false;
             double value = 0.0;
             if (active) {
                 bool stop = false;
                 V3<double> np{0.0, 0.0, 0.0};
                 int bslot = -1;
                 int bid = -1;
-                if (steps == 0) {
-                    stop = start_stops;
-                    if (stop) {
-                        np = V3<double>{st0.nx, st0.ny, st0.nz};
-                        bslot = st0.slot;
-                    }
+                if (start_stops) {
+                    stop = true;
+                    np = V3<double>{st0.nx, st0.ny, st0.nz};
+                    bslot = st0.slot;
                 } else if (!kF32) {
                     stop = !(static_cast<double>(R) > eps);
                     np = np64;
@@ -342,89 +428,6 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                 if (stop) {
                     value = sample + (bslot >= 0 ? boundary_data<DIM>(a, bslot, np, cgrad) : 0.0);
                     done = true;
-                } else {
-                    rng.begin_step(steps);
-                    sample += heat_source<DIM, T>(a, p, R, rng, adj, j);
-                    p = sphere_step<DIM, false, T>(p, R, rng);
-                    ++steps;
-                    if constexpr (kF32) {
-                        need_query = true;
-                        // the walk kernels' lattice step: away from the shell a
-                        // lattice lower bound is the radius (forward and replay
-                        // take the same branches, the lattice is fixed)
-                        if (wv.gd != nullptr && steps < a.max_steps) {
-                            const LatticeSample ls =
-                                lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
-                            const float gb = (ls.d - ls.r) * a.shrink;
-                            if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
-                                R = gb;
-                                need_query = false;
-                            } else if (ls.d <= a.list_t) {
-                                // near the boundary: a query over the node's
-                                // candidate list, when it has one (2D: this
-                                // lane scans it; 3D: the warp, below)
-                                const int v = __ldg(wv.gl + ls.node);
-                                if (v >= 0) {
-                                    if constexpr (DIM == 2) {
-                                        const WideResult q = list_nearest<DIM>(
-                                            wv, list_of(wv, v), list_length(v),
-                                            static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
-                                        const float r = sqrtf(q.best);
-                                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
-                                        slot = q.slot;
-                                    } else {
-                                        packed = v;
-                                    }
-                                    need_query = false;
-                                    listed = true;
-                                }
-                            }
-                        }
-                    } else {
-                        const Nearest<double> q = nearest64<DIM>(
-                            a.s, static_cast<double>(p.x), static_cast<double>(p.y),
-                            static_cast<double>(p.z), dinf());
-                        R = static_cast<T>(sqrt(q.best));
-                        np64 = V3<double>{q.x, q.y, q.z};
-                        slot64 = q.slot;
-                    }
-                }
-            }
-            if constexpr (kF32 && DIM == 3) {
-                const bool want = packed >= 0;
-                if (__any_sync(kFull, want)) {
-                    const WideResult q = warp_list_nearest<DIM>(
-                        wv, want, packed, static_cast<float>(p.x), static_cast<float>(p.y),
-                        static_cast<float>(p.z));
-                    if (want) {
-                        const float r = sqrtf(q.best);
-                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
-                        slot = q.slot;
-                    }
-                }
-            }
-            if constexpr (kF32) {
-                unsigned pending = __ballot_sync(kFull, need_query);
-                queries += __popc(pending) + __popc(__ballot_sync(kFull, listed));
-                float qbest = 0.0f;
-                int qslot = -1;
-                while (pending) {
-                    const int jl = __ffs(pending) - 1;
-                    pending &= pending - 1u;
-                    const float qx = __shfl_sync(kFull, static_cast<float>(p.x), jl);
-                    const float qy = __shfl_sync(kFull, static_cast<float>(p.y), jl);
-                    const float qz =
-                        DIM == 3 ? __shfl_sync(kFull, static_cast<float>(p.z), jl) : 0.0f;
-                    const WideResult r = wide_nearest<DIM, HC>(wv, qx, qy, qz, a.keep, a.exact2);
-                    if (lane == jl) {
-                        qbest = r.best;
-                        qslot = r.slot;
-                    }
-                }
-                if (need_query) {
-                    const float r = sqrtf(qbest);
-                    R = static_cast<T>(qbest > a.shell2 ? r * a.shrink : r);
-                    slot = qslot;
                 }
             }
             if (done) {

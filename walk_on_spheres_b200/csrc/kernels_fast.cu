@@ -76,114 +76,58 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
     FastRng<T> rng(pkey, static_cast<uint32_t>(walk));
 
     while (__any_sync(kFull, active)) {
-        bool done = false;
         bool need_query = false;
         bool listed = false;  // answered from a near-boundary list
         int packed = -1;      // 3D: the list the warp scans for this lane
-        double value = 0.0;
-        if (active) {
-            bool stop = false;
-            V3<double> np{0.0, 0.0, 0.0};
-            int bid = -1;
-            if (steps == 0) {
-                stop = start_stops;
-                if (stop) {
-                    const StartRecord st = a.start[pidx];
-                    np = V3<double>{st.nx, st.ny, st.nz};
-                    bid = st.boundary_id;
-                }
-            } else if (!kF32) {
-                stop = !(static_cast<double>(R) > eps);
-                np = np64;
-                bid = bid64;
-            } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
-                // epsilon shell: FP64 re-projection onto the nearest primitive
-                // (a query that found none is a broken walk: flag it, stop)
-                if (slot < 0) {
-                    bad = true;
-                    stop = true;
-                } else {
-                    const double d2 = reproject64_sq<DIM>(a.s, wv.wide2bin[slot],
-                                                          static_cast<double>(p.x),
-                                                          static_cast<double>(p.y),
-                                                          static_cast<double>(p.z), np, bid);
-                    if (d2 <= eps2) {
-                        stop = true;
-                    } else {
-                        R = static_cast<T>(sqrt(d2));
-                    }
-                }
-            }
-            if (!stop && steps >= a.max_steps) {
-                // step cap: finish at the nearest boundary point
-                // (include/wos/wos.hpp:129-137)
-                ++hits;
-                stop = true;
-                if (kF32) {
-                    if (slot < 0) {
-                        bad = true;
-                    } else {
-                        reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
-                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
-                                         bid);
-                    }
-                } else {
-                    np = np64;
-                    bid = bid64;
-                }
-            }
-            if (stop) {
-                value = static_cast<double>(sample) +
-                        static_cast<double>(weight) * eq.boundary(np, bid);
-                done = true;
-            } else {
-                rng.begin_step(steps);
-                p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
-                ++steps;
-                if constexpr (kF32) {
-                    need_query = true;
-                    if constexpr (HC != kLaneScan) {
-                        // away from the shell a lattice lower bound is a valid
-                        // (smaller) radius and spares the exact query; the step
-                        // that reaches the cap queries, for its nearest point
-                        if (wv.gd != nullptr && steps < a.max_steps) {
-                            const LatticeSample ls =
-                                lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
-                            const float gb = (ls.d - ls.r) * a.shrink;
-                            if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
-                                R = gb;
-                                need_query = false;
-                            } else if (ls.d <= a.list_t) {
-                                // near the boundary: a query over the node's
-                                // candidate list, when it has one; in 2D (a
-                                // few segments) this lane scans it, in 3D the
-                                // warp scans all such lists together below
-                                const int v = __ldg(wv.gl + ls.node);
-                                if (v >= 0) {
-                                    if constexpr (DIM == 2) {
-                                        const WideResult q = list_nearest<DIM>(
-                                            wv, list_of(wv, v), list_length(v),
-                                            static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
-                                        const float r = sqrtf(q.best);
-                                        R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
-                                        slot = q.slot;
-                                    } else {
-                                        packed = v;
-                                    }
-                                    need_query = false;
-                                    listed = true;
+        // One step of every walk in flight (a start point inside the shell
+        // takes none: its walks end where they start).
+        if (active && !start_stops) {
+            rng.begin_step(steps);
+            p = walk_body<DIM, false, T>(eq, p, R, sample, weight, rng, rng, overflow);
+            ++steps;
+            if constexpr (kF32) {
+                need_query = true;
+                if constexpr (HC != kLaneScan) {
+                    // away from the shell a lattice lower bound is a valid
+                    // (smaller) radius and spares the exact query; the step
+                    // that reaches the cap queries, for its nearest point
+                    if (wv.gd != nullptr && steps < a.max_steps) {
+                        const LatticeSample ls =
+                            lattice_sample<DIM>(wv, p.x, p.y, DIM == 3 ? p.z : 0.0f);
+                        const float gb = (ls.d - ls.r) * a.shrink;
+                        if (ls.d >= wv.gratio * ls.r && gb > 0.0f && gb * gb > a.shell2) {
+                            R = gb;
+                            need_query = false;
+                        } else if (ls.d <= a.list_t) {
+                            // near the boundary: a query over the node's
+                            // candidate list, when it has one; in 2D (a
+                            // few segments) this lane scans it, in 3D the
+                            // warp scans all such lists together below
+                            const int v = __ldg(wv.gl + ls.node);
+                            if (v >= 0) {
+                                if constexpr (DIM == 2) {
+                                    const WideResult q = list_nearest<DIM>(
+                                        wv, list_of(wv, v), list_length(v),
+                                        static_cast<float>(p.x), static_cast<float>(p.y), 0.0f);
+                                    const float r = sqrtf(q.best);
+                                    R = static_cast<T>(q.best > a.shell2 ? r * a.shrink : r);
+                                    slot = q.slot;
+                                } else {
+                                    packed = v;
                                 }
+                                need_query = false;
+                                listed = true;
                             }
                         }
                     }
-                } else {
-                    const Nearest<double> q = nearest64<DIM>(
-                        a.s, static_cast<double>(p.x), static_cast<double>(p.y),
-                        static_cast<double>(p.z), dinf());
-                    R = static_cast<T>(sqrt(q.best));
-                    np64 = V3<double>{q.x, q.y, q.z};
-                    bid64 = bid_of<DIM>(a.s, q.slot);
                 }
+            } else {
+                const Nearest<double> q = nearest64<DIM>(
+                    a.s, static_cast<double>(p.x), static_cast<double>(p.y),
+                    static_cast<double>(p.z), dinf());
+                R = static_cast<T>(sqrt(q.best));
+                np64 = V3<double>{q.x, q.y, q.z};
+                bid64 = bid_of<DIM>(a.s, q.slot);
             }
         }
         if constexpr (kF32 && HC == kLaneScan) {
@@ -234,8 +178,67 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                 slot = qslot;
             }
         }
+        // Walks whose new radius is in the epsilon shell, or that reached
+        // the step cap, end in the iteration of their last step, so the lane
+        // steps its next walk in the next iteration.
+        bool done = false;
+        double value = 0.0;
+        if (active) {
+            bool stop = false;
+            V3<double> np{0.0, 0.0, 0.0};
+            int bid = -1;
+            if (start_stops) {
+                stop = true;
+                const StartRecord st = a.start[pidx];
+                np = V3<double>{st.nx, st.ny, st.nz};
+                bid = st.boundary_id;
+            } else if (!kF32) {
+                stop = !(static_cast<double>(R) > eps);
+                np = np64;
+                bid = bid64;
+            } else if (static_cast<float>(R) * static_cast<float>(R) <= a.shell2) {
+                // epsilon shell: FP64 re-projection onto the nearest primitive
+                // (a query that found none is a broken walk: flag it, stop)
+                if (slot < 0) {
+                    bad = true;
+                    stop = true;
+                } else {
+                    const double d2 = reproject64_sq<DIM>(a.s, wv.wide2bin[slot],
+                                                          static_cast<double>(p.x),
+                                                          static_cast<double>(p.y),
+                                                          static_cast<double>(p.z), np, bid);
+                    if (d2 <= eps2) {
+                        stop = true;
+                    } else {
+                        R = static_cast<T>(sqrt(d2));
+                    }
+                }
+            }
+            if (!stop && steps >= a.max_steps) {
+                // step cap: finish at the nearest boundary point
+                // (include/wos/wos.hpp:129-137)
+                ++hits;
+                stop = true;
+                if (kF32) {
+                    if (slot < 0) {
+                        bad = true;
+                    } else {
+                        reproject64<DIM>(a.s, wv.wide2bin[slot], static_cast<double>(p.x),
+                                         static_cast<double>(p.y), static_cast<double>(p.z), np,
+                                         bid);
+                    }
+                } else {
+                    np = np64;
+                    bid = bid64;
+                }
+            }
+            if (stop) {
+                value = static_cast<double>(sample) +
+                        static_cast<double>(weight) * eq.boundary(np, bid);
+                done = true;
+            }
+        }
         if (done) {
-            // Welford update of this lane's statistics
             acc.add(value);
             steps_acc += steps;
         }
@@ -1040,7 +1043,21 @@ FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, in
                    int precision, int device_sms, size_t smem_optin) {
     FastPlan p{};
     p.threads = 256;
-    p.chunk = n_walks < 1024 ? n_walks : 1024;
+    // Walks per task: the longest of 2048 / 1024 / 512 / 256 that still
+    // gives about six tasks per resident warp (32 per SM).  A task's last
+    // walks leave lanes idle, so longer tasks waste less, but a warp's last
+    // task must not run long after the others have finished.  Measured on a
+    // B200: 51k points x 4096 walks runs best at 2048, 4096 points x 2048
+    // walks at 256 (23.8 -> 22.5 ms), 137k points x 1024 walks at 1024.
+    const long long warps = 32LL * (device_sms > 0 ? device_sms : 148);
+    int chunk = 256;
+    for (int c = 2048; c > 256; c /= 2) {
+        if (n_points * ((n_walks + c - 1) / c) >= 6 * warps) {
+            chunk = c;
+            break;
+        }
+    }
+    p.chunk = n_walks < chunk ? n_walks : chunk;
     if (p.chunk < 1) p.chunk = 1;
     p.chunks = (n_walks + p.chunk - 1) / p.chunk;
     p.n_tasks = n_points * p.chunks;
@@ -1053,7 +1070,6 @@ FastPlan plan_fast(const SceneView &s, const WideView &w, long long n_points, in
     p.smem_bytes = p.stage_scene
                        ? static_cast<int>((box_floats + (p.stage_prims ? prim_floats : 0)) * 4)
                        : 0;
-    (void)device_sms;
     p.blocks = 0;  // sized from the occupancy of the chosen kernel at launch
     return p;
 }
