@@ -90,16 +90,17 @@ METHOD_NAMES = {"fast": "FAST_FP32 (FP32 walk + FP64 epsilon shell, FP64 sums)",
 REF_STRIDE = 128
 # walk_fast_kernel on this workload (FAST_FP32), from one ncu capture of each
 # source mode's launch (`python -m walk_on_spheres_b200.benchmarks --profile
-# disk_uniform` / `disk_green`, 512 walks): warp instructions issued
-# (sm__inst_issued.sum) and L2 bytes (lts__t_bytes.sum) per walk step, DRAM
-# bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch (the
-# distance lattice read once and the fields written: the same at any walk
-# count), and the L2 peak the capture implies (lts__t_bytes.sum.per_second
-# over lts__t_sectors.sum.pct_of_peak_sustained_elapsed).
-NCU_PER_STEP = {"uniform": {"issued": 3257663940 / 148740981, "l2_bytes": 7.581465e9 / 148740981},
-                "green": {"issued": 3218209969 / 148751403, "l2_bytes": 7.580572e9 / 148751403}}
+# disk_uniform` / `disk_green`, 2048 walks: tasks of 2048 walks, as in the
+# timed steps): warp instructions issued (sm__inst_issued.sum) and L2 bytes
+# (lts__t_bytes.sum) per walk step, DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) per launch (the distance lattice read once and the
+# fields written: the same at any walk count), and the L2 peak the capture
+# implies (lts__t_bytes.sum.per_second over
+# lts__t_sectors.sum.pct_of_peak_sustained_elapsed).
+NCU_PER_STEP = {"uniform": {"issued": 9751093419 / 595062422, "l2_bytes": 28.298615e9 / 595062422},
+                "green": {"issued": 9584133994 / 595069594, "l2_bytes": 28.265767e9 / 595069594}}
 NCU_DRAM_BYTES_PER_LAUNCH = 22.2e6
-NCU_L2_PEAK_GBS = 1990.496 / 0.05747237
+NCU_L2_PEAK_GBS = 2506.406 / 0.07227765
 ISSUE_SLOTS_PER_SM_CYCLE = 4   # one warp instruction per SM sub-partition per cycle
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
 # 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in

@@ -198,24 +198,23 @@ cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
         return e;
     }
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
-    // list indices are packed above a 6-bit length (int entries); the
-    // lattices hold at most 2^24 nodes, so this never binds
-    band = std::min(band, (1u << 25) - 1u);
     WideView w = wide;
     w.gk = near_list_capacity(w.dim);
     if (const char *env = std::getenv("WOS_NEAR_CAPACITY")) {
         const int k = std::atoi(env);
         if (k >= 1 && k <= 32) w.gk = k;
     }
-    if ((e = gpool.reserve(std::max<size_t>(band, 1) * w.gk * sizeof(int))) != cudaSuccess) {
-        return e;
-    }
+    // K slots per band node bound the packed lists; list offsets sit above
+    // a 5-bit length in an int, so the pool has at most 2^26 slots (nodes
+    // beyond it get no list and query the tree instead)
+    const size_t slots = std::min<size_t>(std::max<size_t>(band, 1) * w.gk, size_t(1) << 26);
+    if ((e = gpool.reserve(slots * sizeof(int))) != cudaSuccess) return e;
     // a point is within r_max of its nearest node; 8 lattice margins cover
     // the FP32 rounding of the distances
     const double rmax = 0.5 * w.gh * std::sqrt(static_cast<double>(w.dim)) * (1.0 + 1e-3);
     const float extra = static_cast<float>(2.0 * rmax + 8.0 * lattice_margin);
     if ((e = launch_near_lists(w, tb, extra, static_cast<int *>(glist.ptr),
-                               static_cast<int *>(gpool.ptr), static_cast<int>(band), count + 1,
+                               static_cast<int *>(gpool.ptr), static_cast<int>(slots), count + 1,
                                sms, stream)) != cudaSuccess) {
         return e;
     }

@@ -58,8 +58,8 @@ struct WideView {
     // of the upper bound D + r of the true distance
     float gratio;
     // Near-boundary candidate lists (null when absent): gl[node] is -1 or
-    // (list index << 6) | length, the list's wide slots at
-    // gpool + index * gk (-1 past its length).  The list holds every primitive within
+    // (offset << 5) | (length - 1), the list's wide slots at gpool + offset,
+    // lists packed end to end (at most gk slots each).  The list holds every primitive within
     // d(node) + 2 r_max of the node (r_max the largest distance from a point
     // to its nearest node), so it holds the nearest primitive of every point
     // whose nearest node this is.
@@ -214,11 +214,11 @@ __device__ __forceinline__ float slot_dist(const WideView &w, int s, float px, f
     return eberly32(px, py, pz, rec);
 }
 
-// A node's packed list entry gl[node] = (list index << 6) | length, or -1.
+// A node's packed list entry gl[node] = (offset << 5) | (length - 1), or -1.
 __device__ __forceinline__ const int *list_of(const WideView &w, int packed) {
-    return w.gpool + static_cast<long long>(packed >> 6) * w.gk;
+    return w.gpool + (packed >> 5);
 }
-__device__ __forceinline__ int list_length(int packed) { return packed & 63; }
+__device__ __forceinline__ int list_length(int packed) { return (packed & 31) + 1; }
 
 // Closest primitive among a near-boundary candidate list of k wide slots,
 // found by this lane alone; the first minimum in list order (ascending
@@ -261,7 +261,7 @@ __device__ __forceinline__ WideResult warp_list_nearest(const WideView &w, bool 
     }
     const int total = __shfl_sync(kAll, inc, 31);
     const int off = inc - k;  // this lane's first pair
-    const int first = want ? (packed >> 6) * w.gk : 0;  // < 2^30: index < 2^24, gk <= 32
+    const int first = want ? (packed >> 5) : 0;  // the list's offset in the pool
     unsigned long long best = kNone;
     for (int c = 0; c < total; c += 32) {
         const int g = c + lane;  // the pair this lane measures

@@ -218,14 +218,15 @@ inline int near_list_capacity(int) { return 16; }
 // with 0 <= value <= t gets the wide slots of all primitives within its exact
 // FP32 distance plus `extra` (2 r_max and a rounding margin), if there are
 // at most near_list_capacity of them.  `count` (device) receives the number
-// of such nodes first (band pass, pool null), then the lists are written.
+// of such nodes first (band pass); the lists are then written end to end into
+// the pool's `pool_slots` slots, `counter` counting the slots used.
 cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaStream_t stream);
 // The primitive records one slot after another (WideView::aos) for the list
 // scans: prim_aos_bytes(w) bytes.
 size_t prim_aos_bytes(const WideView &w);
 cudaError_t launch_prim_aos(const WideView &w, float *aos, cudaStream_t stream);
 cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
-                              int pool_lists, unsigned *counter, int sms, cudaStream_t stream);
+                              int pool_slots, unsigned *counter, int sms, cudaStream_t stream);
 cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin, float *out,
                              int sms, void *scratch, double tol, cudaStream_t stream);
 // lattice_bound at each point (FP32), NaN where the scene has no lattice.

@@ -875,10 +875,12 @@ __global__ void near_band_kernel(const float *__restrict__ gd, long long n, floa
 }
 
 // One band node per warp: its exact FP32 distance d, then every primitive
-// within d + extra, kept as its list when there are at most K.
+// within d + extra, kept as its list when there are at most K.  Lists are
+// packed end to end, so the pool holds about the average length per node
+// rather than K: what the walks touch stays small enough for L2.
 template <int DIM, int HC>
 __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, float extra,
-                                                         int *gl, int *pool, int pool_lists,
+                                                         int *gl, int *pool, int pool_slots,
                                                          unsigned *counter) {
     __shared__ int s_list[8][32];
     const int lane = threadIdx.x & 31;
@@ -904,17 +906,18 @@ __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, fl
         const float radius = sqrtf(q.best) * (1.0f + 0x1p-16f) + extra;
         const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list[wib], K);
         __syncwarp();
+        // the list goes to the next cnt slots of the pool (lists end to end)
         int idx = -1;
         if (cnt >= 1 && cnt <= K) {
-            if (lane == 0) idx = static_cast<int>(atomicAdd(counter, 1u));
-            idx = __shfl_sync(kFull, idx, 0);
-            if (idx >= pool_lists) idx = -1;  // cannot happen: the pool holds the band
+            unsigned at = 0;
+            if (lane == 0) at = atomicAdd(counter, static_cast<unsigned>(cnt));
+            at = __shfl_sync(kFull, at, 0);
+            // never short: the pool holds K slots per band node (at most 2^26)
+            if (static_cast<long long>(at) + cnt <= pool_slots) idx = static_cast<int>(at);
         }
-        if (idx >= 0 && lane < K) {
-            pool[static_cast<long long>(idx) * K + lane] = lane < cnt ? s_list[wib][lane] : -1;
-        }
-        // packed entry: (list index << 6) | length (index < 2^24, length <= 32)
-        if (lane == 0) gl[node] = idx >= 0 ? (idx << 6) | cnt : -1;
+        if (idx >= 0 && lane < cnt) pool[static_cast<long long>(idx) + lane] = s_list[wib][lane];
+        // packed entry: (offset << 5) | (length - 1), offset < 2^26
+        if (lane == 0) gl[node] = idx >= 0 ? (idx << 5) | (cnt - 1) : -1;
         __syncwarp();
     }
 }
@@ -953,7 +956,7 @@ cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaSt
 }
 
 cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
-                              int pool_lists, unsigned *counter, int sms, cudaStream_t stream) {
+                              int pool_slots, unsigned *counter, int sms, cudaStream_t stream) {
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
@@ -962,10 +965,10 @@ cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, 
         constexpr int HC = decltype(h)::value;
         if (w.dim == 2) {
             near_lists_kernel<2, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-                w, t, extra, gl, pool, pool_lists, counter);
+                w, t, extra, gl, pool, pool_slots, counter);
         } else {
             near_lists_kernel<3, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-                w, t, extra, gl, pool, pool_lists, counter);
+                w, t, extra, gl, pool, pool_slots, counter);
         }
         return cudaGetLastError();
     });
