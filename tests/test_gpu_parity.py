@@ -144,6 +144,23 @@ def test_solve_points_matches_grid(solver):
     assert np.array_equal(r.mean[ins], g.mean.ravel()[ins])
 
 
+def test_solve_points_rejects_non_finite_points(solver):
+    """A NaN or infinite start point (or heat probe) is refused on the host
+    with a clear message, before anything reaches the device."""
+    from walk_on_spheres_b200._lib import WosError
+    from walk_on_spheres_b200.heat import HeatProblem
+    solver.set_mesh(mesh_by_name("annulus"))
+    for bad in (np.nan, np.inf):
+        pts = np.array([[0.5, 0.0], [bad, 0.1]])
+        with pytest.raises(WosError, match="point coordinates must be finite"):
+            solver.solve_points("laplace", pts, N_walks=16, method="fast")
+        with pytest.raises(WosError, match="probe coordinates must be finite"):
+            HeatProblem(solver, pts, N_walks=16).forward(1.0, (0.5, 0.0), 0.1)
+    # the context stays usable
+    r = solver.solve_points("laplace", np.array([[0.5, 0.0]]), N_walks=16, method="fast")
+    assert r.location[0] in (0, 1, 2)
+
+
 def test_sharded_solver_matches_grid(solver):
     """The per-shard GPU solver (walk_on_spheres_b200.parallel) reproduces the
     grid sweep point for point: same coordinates, same global-index seeds."""

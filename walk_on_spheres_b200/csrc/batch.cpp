@@ -305,6 +305,10 @@ int wos_batch::plan() {
                         static_cast<uint8_t *>(f_loc.ptr) + b.point_begin};
         // boundary tolerance 1e-10 * max(1, mesh extents), include/wos/runner.hpp:86-88
         it.btol = 1e-10 * m.scene.scale;
+        // FAST_FP32 start radii from FP32 bounds away from the shell, as in
+        // a lone solve (FastStart)
+        it.exact_below = precision == 32 ? std::max(effective_epsilon(b.p), it.btol) : -1.0;
+        it.start_margin = fp32_distance_margin(m.scene.bbox, dim);
         it.max_ray_attempts = b.p.max_ray_attempts;
         it.precision = precision;
         it.point_begin = b.point_begin;

@@ -284,7 +284,7 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
     wide.gh = static_cast<float>(step);
     wide.ginv = static_cast<float>(1.0 / step);
     // FP32 primitive distances carry a few ulps of the largest coordinate
-    const float margin = static_cast<float>(4e-6 * std::max(mag, ext));
+    const float margin = fp32_distance_margin(h.bbox, h.dim);
     lattice_margin = margin;
     const size_t count = static_cast<size_t>(n[0]) * n[1] * n[2];
     cudaError_t e = lattice.reserve(sizeof(float) * count);
@@ -473,8 +473,15 @@ int wos_context::run(const wos_params &p, const PointSet &ps, Fields out,
     auto *ctr = static_cast<DeviceCounters *>(counters.ptr);
 
     WOS_CUDA(this, cudaEventRecord(events[0], stream), "event");
+    FastStart fs;
+    if (p.method == WOS_METHOD_FAST_FP32) {
+        fs.on = true;
+        fs.w = wide;
+        fs.exact_below = std::max(eps, btol);
+        fs.margin = fp32_distance_margin(scene.bbox, dim);
+    }
     WOS_CUDA(this, launch_classify(view, ps, p.seed, p.max_ray_attempts, btol,
-                                   eq, out, loc, st, ctr, stream),
+                                   eq, out, loc, st, ctr, stream, fs),
              "classification kernel");
     WOS_CUDA(this, cudaEventRecord(events[1], stream), "event");
     if (p.method == WOS_METHOD_PLAIN_FP64) {
@@ -647,6 +654,11 @@ extern "C" int wos_solve_points(wos_context *ctx, const wos_params *params, cons
     if (!ctx) return fail(nullptr, WOS_ERR_INVALID, "null context");
     std::string err = check_params(ctx, params);
     if (err.empty() && (!points || n < 0)) err = "null points";
+    // a non-finite point has no place in the domain; reject it here rather
+    // than hand it to the traversals
+    for (long long i = 0; err.empty() && i < n * ctx->scene.dim; ++i) {
+        if (!std::isfinite(points[i])) err = "point coordinates must be finite";
+    }
     if (!err.empty()) return fail(ctx, WOS_ERR_INVALID, "wos_solve_points: " + err);
     cudaSetDevice(ctx->device);
     const int dim = ctx->scene.dim;

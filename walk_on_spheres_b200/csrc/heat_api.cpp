@@ -114,6 +114,11 @@ std::string check_heat(const wos_context *ctx, const wos_params *p,
         }
     }
     if (n < 0 || (n > 0 && !probes)) return "null probes";
+    // a non-finite probe has no place in the domain; reject it here rather
+    // than hand it to the traversals
+    for (long long i = 0; i < n * ctx->scene.dim; ++i) {
+        if (!std::isfinite(probes[i])) return "probe coordinates must be finite";
+    }
     return std::string();
 }
 

@@ -9,13 +9,45 @@
 
 namespace wosb {
 
+// Absolute error margin of FP32 primitive distances in a scene with this
+// bounding box: a few ulps of its largest coordinate or extent.
+inline float fp32_distance_margin(const double bbox[6], int dim) {
+    double ext = 0.0, mag = 0.0;
+    for (int k = 0; k < dim; ++k) {
+        const double lo = bbox[2 * k], hi = bbox[2 * k + 1];
+        ext = ext > hi - lo ? ext : hi - lo;
+        mag = mag > (lo < 0 ? -lo : lo) ? mag : (lo < 0 ? -lo : lo);
+        mag = mag > (hi < 0 ? -hi : hi) ? mag : (hi < 0 ? -hi : hi);
+    }
+    return static_cast<float>(4e-6 * (mag > ext ? mag : ext));
+}
+
+// FAST_FP32 start radii.  A walk only needs its start radius to be a lower
+// bound of the boundary distance; the exact FP64 distance matters only where
+// it decides something: the boundary class (radius <= boundary tolerance)
+// and a start inside the epsilon shell.  With `fast` set, each point first
+// gets a conservative FP32 bound from the wide tree (the lattice build's
+// query, shrunk by 2^-10 and `margin`); points whose bound exceeds
+// `exact_below` (the larger of epsilon and the boundary tolerance) keep it
+// as their start radius and skip the exact query, whose cost on
+// sphere-like meshes grows with the number of nearly equidistant
+// primitives.  Locations and which walks start inside the shell are the
+// same as with exact radii.
+struct FastStart {
+    bool on = false;
+    WideView w{};
+    double exact_below = 0.0;
+    float margin = 0.0f;
+};
+
 // Start points, classification and boundary values for every point of `ps`
 // (include/wos/runner.hpp:170-206).  Writes location, start records and the
 // fields of non-inside points.
 cudaError_t launch_classify(const SceneView &s, const PointSet &ps, uint64_t seed,
                             int max_ray_attempts, double boundary_tolerance, EqDesc eq,
                             Fields out, uint8_t *location, StartRecord *start,
-                            DeviceCounters *counters, cudaStream_t stream);
+                            DeviceCounters *counters, cudaStream_t stream,
+                            const FastStart &fast = FastStart{});
 
 // PLAIN_FP64: every walk of every inside point on the point's reference
 // xoshiro256++ streams, in the reference order (include/wos/wos.hpp:54-191).
@@ -92,6 +124,8 @@ struct BatchItem {
     EqDesc eq;
     Fields out;
     double btol;             // boundary tolerance of the classification
+    double exact_below;      // FastStart::exact_below, or < 0: exact start radii
+    float start_margin;      // FastStart::margin
     int max_ray_attempts;
     int precision;           // 32 / 64
     long long point_begin;   // first point of the solve in the batch's point order

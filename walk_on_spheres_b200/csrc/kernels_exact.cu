@@ -45,24 +45,38 @@ __device__ int classify_3d(const SceneView &s, const double *p, double bdist, do
 }
 
 // Start point, location and (non-inside) fields of point t of `ps`
-// (include/wos/runner.hpp:170-206).
+// (include/wos/runner.hpp:170-206).  A lower bound `lo` of the point's
+// distance above `exact_below` (FastStart) becomes the start radius without
+// the exact query; its start record then has no nearest point (slot -1),
+// which no walk reads: such a point is neither on the boundary nor inside the
+// shell.
 template <int DIM>
 __device__ __forceinline__ void classify_point(const SceneView &s, const PointSet &ps,
                                                long long t, uint64_t seed, int max_ray_attempts,
                                                double btol, const EqDesc &eq, const Fields &out,
                                                uint8_t *location, StartRecord *start,
-                                               DeviceCounters *ctr) {
+                                               DeviceCounters *ctr, double lo = -1.0,
+                                               double exact_below = 0.0) {
     double p[3];
     uint64_t linear;
     point_at(ps, t, p[0], p[1], p[2], linear);
-    const Nearest<double> q = nearest64<DIM>(s, p[0], p[1], p[2], dinf());
     StartRecord st;
-    st.radius = sqrt(q.best);
-    st.nx = q.x;
-    st.ny = q.y;
-    st.nz = DIM == 3 ? q.z : 0.0;
-    st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
-    st.slot = q.slot;
+    if (exact_below >= 0.0 && lo > exact_below) {
+        st.radius = lo;
+        st.nx = p[0];
+        st.ny = p[1];
+        st.nz = DIM == 3 ? p[2] : 0.0;
+        st.boundary_id = -1;
+        st.slot = -1;
+    } else {
+        const Nearest<double> q = nearest64<DIM>(s, p[0], p[1], p[2], dinf());
+        st.radius = sqrt(q.best);
+        st.nx = q.x;
+        st.ny = q.y;
+        st.nz = DIM == 3 ? q.z : 0.0;
+        st.boundary_id = (DIM == 2 && q.slot >= 0) ? s.segid[q.slot].x : -1;
+        st.slot = q.slot;
+    }
     int where;
     if (DIM == 2) {
         where = st.radius <= btol ? 2 : (winding_number(s, p[0], p[1]) != 0 ? 1 : 0);
@@ -101,26 +115,102 @@ __global__ void __launch_bounds__(kExactThreads)
     }
 }
 
+// FastStart lower bounds of the points of a warp: lane j's point (when
+// `want`) is queried by the whole warp with the lattice build's conservative
+// wide-tree query, on scene w_of(j).  Returns this lane's bound, or -1.
+template <int DIM, int HC, class WOf, class MarginOf>
+__device__ __forceinline__ float start_bounds(bool want, double x, double y, double z, WOf w_of,
+                                              MarginOf margin_of) {
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr float kShrink = 1.0f - 0x1p-10f;
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    float lo = -1.0f;
+    unsigned todo = __ballot_sync(kAll, want);
+    while (todo) {
+        const int j = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        const float qx = __shfl_sync(kAll, static_cast<float>(x), j);
+        const float qy = __shfl_sync(kAll, static_cast<float>(y), j);
+        const float qz = DIM == 3 ? __shfl_sync(kAll, static_cast<float>(z), j) : 0.0f;
+        // both lookups may shuffle: every lane takes them here, converged
+        const WideView &wj = w_of(j);
+        const float mj = margin_of(j);
+        const WideResult q = wide_nearest<DIM, HC>(wj, qx, qy, qz, kShrink * kShrink, 0.0f);
+        if (lane == j && q.slot >= 0) {
+            // the rounding of the point to FP32 and of the distance
+            // arithmetic stay within the margin (the lattice's bound)
+            const float d = (sqrtf(q.best) * kShrink - mj) * (1.0f - 0x1p-20f);
+            lo = d > 0.0f ? d : 0.0f;
+        }
+    }
+    return lo;
+}
+
+// classify_kernel with FastStart: one warp per 32 consecutive points.
+template <int DIM, int HC>
+__global__ void __launch_bounds__(kExactThreads)
+    classify_fast_kernel(SceneView s, WideView w, PointSet ps, uint64_t seed, int max_ray_attempts,
+                         double btol, double exact_below, float margin, EqDesc eq, Fields out,
+                         uint8_t *location, StartRecord *start, DeviceCounters *ctr) {
+    const long long lane = threadIdx.x & 31;
+    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < ps.n; base += warps * 32) {
+        const long long t = base + lane;
+        const bool valid = t < ps.n;
+        double x = 0.0, y = 0.0, z = 0.0;
+        uint64_t linear = 0;
+        if (valid) point_at(ps, t, x, y, z, linear);
+        const float lo = start_bounds<DIM, HC>(
+            valid, x, y, z, [&](int) -> const WideView & { return w; },
+            [&](int) { return margin; });
+        if (valid) {
+            classify_point<DIM>(s, ps, t, seed, max_ray_attempts, btol, eq, out, location, start,
+                                ctr, static_cast<double>(lo), exact_below);
+        }
+    }
+}
+
 // Classification of a batch: global point g in [base, base + n) belongs to
-// the item with the largest point_begin <= g.
+// the item with the largest point_begin <= g.  One warp per 32 consecutive
+// points, so FAST_FP32 items can take FastStart bounds (items[i].exact_below
+// >= 0), each point on its own item's scene.
 template <int DIM>
 __global__ void __launch_bounds__(kExactThreads)
     classify_batch_kernel(const BatchItem *__restrict__ items, int n_items, long long base,
                           long long n) {
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < n;
-         t += stride) {
+    const long long lane = threadIdx.x & 31;
+    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    for (long long first = warp * 32; first < n; first += warps * 32) {
+        const long long t = first + lane;
+        const bool valid = t < n;
         const long long g = base + t;
-        int lo = 0, hi = n_items - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].point_begin <= g) lo = mid;
-            else hi = mid - 1;
+        int lo_i = 0;
+        if (valid) {
+            int hi = n_items - 1;
+            while (lo_i < hi) {
+                const int mid = (lo_i + hi + 1) >> 1;
+                if (items[mid].point_begin <= g) lo_i = mid;
+                else hi = mid - 1;
+            }
         }
-        const BatchItem &it = items[lo];
-        classify_point<DIM>(it.a.s, it.a.ps, g - it.point_begin, it.a.seed, it.max_ray_attempts,
-                            it.btol, it.eq, it.out, const_cast<uint8_t *>(it.a.location),
-                            const_cast<StartRecord *>(it.a.start), it.a.ctr);
+        const BatchItem &it = items[lo_i];
+        double x = 0.0, y = 0.0, z = 0.0;
+        uint64_t linear = 0;
+        if (valid) point_at(it.a.ps, g - it.point_begin, x, y, z, linear);
+        const bool want = valid && it.exact_below >= 0.0;
+        const float lo = start_bounds<DIM, kHeightAny>(
+            want, x, y, z,
+            [&](int j) -> const WideView & { return items[__shfl_sync(0xffffffffu, lo_i, j)].a.w; },
+            [&](int j) { return items[__shfl_sync(0xffffffffu, lo_i, j)].start_margin; });
+        if (valid) {
+            classify_point<DIM>(it.a.s, it.a.ps, g - it.point_begin, it.a.seed,
+                                it.max_ray_attempts, it.btol, it.eq, it.out,
+                                const_cast<uint8_t *>(it.a.location),
+                                const_cast<StartRecord *>(it.a.start), it.a.ctr,
+                                static_cast<double>(lo), it.exact_below);
+        }
     }
 }
 
@@ -274,9 +364,25 @@ void launch_plain_dim(const SceneView &s, const PointSet &ps, uint64_t seed, EqD
 cudaError_t launch_classify(const SceneView &s, const PointSet &ps, uint64_t seed,
                             int max_ray_attempts, double btol, EqDesc eq, Fields out,
                             uint8_t *location, StartRecord *start, DeviceCounters *counters,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, const FastStart &fast) {
     if (ps.n <= 0) return cudaSuccess;
     const int blocks = blocks_for(ps.n, kExactThreads);
+    if (fast.on && fast.w.n > 0) {
+        const WideView &w = fast.w;
+        return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
+            constexpr int HC = decltype(h)::value;
+            if (s.dim == 2) {
+                classify_fast_kernel<2, HC><<<blocks, kExactThreads, 0, stream>>>(
+                    s, w, ps, seed, max_ray_attempts, btol, fast.exact_below, fast.margin, eq,
+                    out, location, start, counters);
+            } else {
+                classify_fast_kernel<3, HC><<<blocks, kExactThreads, 0, stream>>>(
+                    s, w, ps, seed, max_ray_attempts, btol, fast.exact_below, fast.margin, eq,
+                    out, location, start, counters);
+            }
+            return cudaGetLastError();
+        });
+    }
     if (s.dim == 2) {
         classify_kernel<2><<<blocks, kExactThreads, 0, stream>>>(s, ps, seed, max_ray_attempts,
                                                                  btol, eq, out, location, start,

@@ -129,8 +129,16 @@ extern "C" int wos_solve_grid_device_noalloc(wos_context *ctx, const wos_params 
     const double btol = 1e-10 * ctx->scene.scale;
     wosb::Fields out{mean, variance, standard_error, mean_steps, location};
     cudaEventRecord(ctx->events[0], s);
+    // the same start radii as wos_solve_grid_device (FastStart for FAST_FP32)
+    wosb::FastStart fs;
+    if (p->method == WOS_METHOD_FAST_FP32) {
+        fs.on = true;
+        fs.w = ctx->wide;
+        fs.exact_below = std::max(eps, btol);
+        fs.margin = wosb::fp32_distance_margin(ctx->scene.bbox, ctx->scene.dim);
+    }
     e = wosb::launch_classify(ctx->view, ps, p->seed, p->max_ray_attempts, btol, eq, out, loc,
-                              start, ctr, s);
+                              start, ctr, s, fs);
     if (e != cudaSuccess) return fail(ctx, WOS_ERR_CUDA, std::string("classification kernel: ") + cudaGetErrorString(e));
     cudaEventRecord(ctx->events[1], s);
     if (!fast) {
