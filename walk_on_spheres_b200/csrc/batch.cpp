@@ -269,9 +269,28 @@ int wos_batch::plan() {
                                   near_list_threshold(m.dev.wide, effective_epsilon(b.p),
                                                       std::ldexp(m.scene.scale, -16)));
     }
+    // every mesh's band count first, one synchronisation, then the lists
+    std::vector<size_t> need;
     for (size_t k = 0; k < meshes.size(); ++k) {
-        WOS_CUDA(ctx, meshes[k]->dev.ensure_lists(list_t[k], ctx->sms, ctx->stream),
-                 "near-boundary lists");
+        if (!meshes[k]->dev.lists_needed(list_t[k])) continue;
+        WOS_CUDA(ctx, meshes[k]->dev.lists_count(list_t[k], ctx->stream), "near-boundary band");
+        need.push_back(k);
+    }
+    if (!need.empty()) {
+        WOS_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "near-boundary band");
+        // all counts before any build is queued (a plain copy may wait for
+        // work on the stream)
+        std::vector<unsigned> band(need.size(), 0);
+        for (size_t i = 0; i < need.size(); ++i) {
+            WOS_CUDA(ctx, cudaMemcpy(&band[i], meshes[need[i]]->dev.gcount.ptr, sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost),
+                     "near-boundary band");
+        }
+        for (size_t i = 0; i < need.size(); ++i) {
+            const size_t k = need[i];
+            WOS_CUDA(ctx, meshes[k]->dev.lists_build(list_t[k], band[i], ctx->sms, ctx->stream),
+                     "near-boundary lists");
+        }
     }
     families.clear();
     for (int i = 0; i < n; ++i) {

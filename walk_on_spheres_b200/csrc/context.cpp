@@ -179,25 +179,26 @@ cudaError_t SceneDevice::upload(const HostScene &h, cudaStream_t stream) {
     return build_lattice(h, stream);
 }
 
-cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
-    if (wide.gd == nullptr || !(t > 0.0f)) return cudaSuccess;
+bool SceneDevice::lists_needed(float t) const {
+    if (wide.gd == nullptr || !(t > 0.0f)) return false;
     if (const char *env = std::getenv("WOS_NEAR_LISTS")) {
-        if (std::string(env) == "0") return cudaSuccess;
+        if (std::string(env) == "0") return false;
     }
-    if (wide.gl != nullptr && list_built >= t) return cudaSuccess;
+    return !(wide.gl != nullptr && list_built >= t);
+}
+
+cudaError_t SceneDevice::lists_count(float t, cudaStream_t stream) {
     const float tb = t * 1.25f;
     const size_t nodes = static_cast<size_t>(wide.gn[0]) * wide.gn[1] * wide.gn[2];
     cudaError_t e = glist.reserve(nodes * sizeof(int));
     if (e != cudaSuccess) return e;
     if ((e = gcount.reserve(2 * sizeof(unsigned))) != cudaSuccess) return e;
+    return launch_near_band(wide, tb, static_cast<unsigned *>(gcount.ptr), stream);
+}
+
+cudaError_t SceneDevice::lists_build(float t, unsigned band, int sms, cudaStream_t stream) {
+    const float tb = t * 1.25f;
     auto *count = static_cast<unsigned *>(gcount.ptr);
-    if ((e = launch_near_band(wide, tb, count, stream)) != cudaSuccess) return e;
-    unsigned band = 0;
-    if ((e = cudaMemcpyAsync(&band, count, sizeof(band), cudaMemcpyDeviceToHost, stream)) !=
-        cudaSuccess) {
-        return e;
-    }
-    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     WideView w = wide;
     w.gk = near_list_capacity(w.dim);
     if (const char *env = std::getenv("WOS_NEAR_CAPACITY")) {
@@ -208,7 +209,8 @@ cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
     // a 5-bit length in an int, so the pool has at most 2^26 slots (nodes
     // beyond it get no list and query the tree instead)
     const size_t slots = std::min<size_t>(std::max<size_t>(band, 1) * w.gk, size_t(1) << 26);
-    if ((e = gpool.reserve(slots * sizeof(int))) != cudaSuccess) return e;
+    cudaError_t e = gpool.reserve(slots * sizeof(int));
+    if (e != cudaSuccess) return e;
     // a point is within r_max of its nearest node; 8 lattice margins cover
     // the FP32 rounding of the distances
     const double rmax = 0.5 * w.gh * std::sqrt(static_cast<double>(w.dim)) * (1.0 + 1e-3);
@@ -226,6 +228,19 @@ cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
     wide.aos = static_cast<const float4 *>(gaos.ptr);
     list_built = tb;
     return cudaSuccess;
+}
+
+cudaError_t SceneDevice::ensure_lists(float t, int sms, cudaStream_t stream) {
+    if (!lists_needed(t)) return cudaSuccess;
+    cudaError_t e = lists_count(t, stream);
+    if (e != cudaSuccess) return e;
+    unsigned band = 0;
+    if ((e = cudaMemcpyAsync(&band, gcount.ptr, sizeof(band), cudaMemcpyDeviceToHost, stream)) !=
+        cudaSuccess) {
+        return e;
+    }
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    return lists_build(t, band, sms, stream);
 }
 
 void SceneDevice::set_views(const HostScene &h) {

@@ -55,6 +55,13 @@ struct SceneDevice {
     // a scene without a lattice, or WOS_NEAR_LISTS=0, has none.  Waits for
     // the stream once (the band size sizes the list pool).
     cudaError_t ensure_lists(float t, int sms, cudaStream_t stream);
+    // ensure_lists in two halves, so a batch can count the bands of all its
+    // meshes before one synchronisation: lists_needed(t) says whether lists
+    // up to t are missing; lists_count(t) enqueues the band count (into
+    // gcount); lists_build(t, band) sizes the pool and builds the lists.
+    bool lists_needed(float t) const;
+    cudaError_t lists_count(float t, cudaStream_t stream);
+    cudaError_t lists_build(float t, unsigned band, int sms, cudaStream_t stream);
     DeviceBuffer glist, gpool, gcount, gaos;
     float list_built = -1.0f;  // the value up to which lists were built
     float lattice_margin = 0.0f;
