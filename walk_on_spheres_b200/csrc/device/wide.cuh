@@ -59,10 +59,10 @@ struct WideView {
     float gratio;
     // Near-boundary candidate lists (null when absent): gl[node] is -1 or
     // (offset << 5) | (length - 1), the list's wide slots at gpool + offset,
-    // lists packed end to end (at most gk slots each).  The list holds every primitive within
-    // d(node) + 2 r_max of the node (r_max the largest distance from a point
-    // to its nearest node), so it holds the nearest primitive of every point
-    // whose nearest node this is.
+    // lists packed end to end (at most gk slots each).  The list holds every
+    // primitive within d(node) + 2 r_max of the node (r_max the largest
+    // distance from a point to its nearest node), so it holds the nearest
+    // primitive of every point whose nearest node this is.
     const int *gl;
     const int *gpool;
     int gk;
