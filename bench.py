@@ -16,8 +16,9 @@ standard error against the FP64 estimator: walks/s * var_fp64 / var_fast
 standard error is proportional to var / throughput).  Device time is taken
 with CUDA events on the library's stream around each solve; the L2 cache is
 flushed (256 MiB write) between steps, outside the events.  `e2e` is the same
-metric through the C ABI with host buffers (mesh upload + BVH build + solve +
-copy of the five result fields to the host, both modes), wall-clocked.
+metric through the C ABI with host buffers (mesh upload + BVH build on the
+device + solve + copy of the five result fields into pinned host memory,
+both modes), wall-clocked.
 
 `closest_point_queries_per_s` counts the walk steps that ran a BVH
 closest-point query; the other steps took their radius from the distance
@@ -216,28 +217,13 @@ def workload_mesh():
     return meshes.circle(segments=1024)
 
 
-def scene_upload_bytes(mesh) -> int:
-    """Bytes wos_set_mesh copies host->device for a 2D mesh: binary-tree boxes
-    (2^(D+1) x 4 doubles), FP64 segments (4 doubles) and {boundary id,
-    primitive} per slot, the 32-wide tree's child blocks, its primitive
-    blocks (5 floats per slot), wide-to-binary slot map, height offsets and
-    vertex ids per slot.  The distance lattice is built on the device."""
-    from walk_on_spheres_b200 import _lib
-    import ctypes as C
-    L = _lib.lib()
-    d, H, E = C.c_int(), C.c_int(), C.c_int()
-    verts = np.ascontiguousarray(mesh.verts)
-    prims = np.ascontiguousarray(mesh.prims, dtype=np.int32)
-    vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-    L.wos_build_bvh.restype = C.c_int
-    L.wos_build_bvh(2, vp(verts), verts.shape[0], vp(prims), prims.shape[0], 0, C.byref(d),
-                    None, None)
-    L.wos_build_wide_bvh(2, vp(verts), verts.shape[0], vp(prims), prims.shape[0], C.byref(H),
-                         C.byref(E), None, None, None)
-    n, D = mesh.n_prims, d.value
-    npad = (n + 31) // 32 * 32
-    return ((2 ** (D + 1)) * 32 + n * 32 + n * 8 + E.value * 4 + npad * 20 + npad * 4 + 32
-            + n * 8)
+def mesh_upload_bytes(mesh) -> int:
+    """Bytes wos_set_mesh copies host->device: the vertices, primitives and
+    boundary ids, from which the trees and the distance lattice are built on
+    the device (plus the wide tree's split plan, a few hundred bytes, and
+    the 8 height offsets, not counted)."""
+    return int(mesh.verts.nbytes + np.asarray(mesh.prims, dtype=np.int32).nbytes +
+               np.asarray(mesh.boundary_ids, dtype=np.int32).nbytes)
 
 
 def hbm_peak():
@@ -606,7 +592,9 @@ def gpu_arm(args, rank, world, local):
     from walk_on_spheres_b200 import _lib
     L = _lib.lib()
     m_loc = end - start
-    host = [np.empty(m_loc) for _ in range(4)] + [np.empty(m_loc, dtype=np.uint8)]
+    # the step's results land in pinned host memory
+    host = ([torch.empty(m_loc, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+            + [torch.empty(m_loc, dtype=torch.uint8, pin_memory=True).numpy()])
 
     def host_step():
         solver.set_mesh(mesh)
@@ -639,7 +627,7 @@ def gpu_arm(args, rank, world, local):
     e2e_s, (e2e_walks,) = reduce_over_ranks(dist, dev, e2e_s, [e2e_walks])
     e2e_value = e2e_walks / e2e_s * var_ratio
     pts_bytes = (m_loc * 2 * 8 + m_loc * 8) if strong else 0
-    h2d = scene_upload_bytes(mesh) + mesh.verts.nbytes + mesh.prims.nbytes + pts_bytes
+    h2d = mesh_upload_bytes(mesh) + pts_bytes
     d2h = len(MODES) * m_loc * (4 * 8 + 1)
 
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
