@@ -185,12 +185,35 @@ int wos_batch::prepare() {
         }
     } join{pool};
     cudaSetDevice(ctx->device);
-    for (size_t i = 0; i < todo.size(); ++i) {
+    // meshes go to the device in the order their builds finish (the largest
+    // ready one first), so the device starts on the small meshes while the
+    // large ones still build
+    std::vector<char> taken(todo.size(), 0);
+    for (size_t c = 0; c < todo.size(); ++c) {
+        size_t i = 0;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv.wait(lk, [&] { return done[i] != 0; });
+            cv.wait(lk, [&] {
+                for (size_t q = 0; q < todo.size(); ++q) {
+                    if (done[q] && !taken[q]) {
+                        i = q;
+                        return true;
+                    }
+                }
+                return false;
+            });
         }
-        if (!errs[i].empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + errs[i]);
+        taken[i] = 1;
+        if (!errs[i].empty()) {
+            // report the first failing mesh in build order, as a serial build would
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] {
+                return std::all_of(done.begin(), done.end(), [](char d) { return d != 0; });
+            });
+            for (size_t q = 0; q < todo.size(); ++q) {
+                if (!errs[q].empty()) return fail(ctx, WOS_ERR_MESH, "Mesh: " + errs[q]);
+            }
+        }
         BatchMesh &m = *todo[i];
         WOS_CUDA(ctx, m.dev.upload(m.scene, ctx->stream), "batch mesh upload");
         m.built = true;

@@ -190,7 +190,7 @@ bool SceneDevice::lists_needed(float t) const {
 cudaError_t SceneDevice::lists_count(float t, cudaStream_t stream) {
     const float tb = t * 1.25f;
     const size_t nodes = static_cast<size_t>(wide.gn[0]) * wide.gn[1] * wide.gn[2];
-    cudaError_t e = glist.reserve(nodes * sizeof(int));
+    cudaError_t e = glist.reserve(nodes * sizeof(int2));
     if (e != cudaSuccess) return e;
     if ((e = gcount.reserve(2 * sizeof(unsigned))) != cudaSuccess) return e;
     return launch_near_band(wide, tb, static_cast<unsigned *>(gcount.ptr), stream);
@@ -215,15 +215,23 @@ cudaError_t SceneDevice::lists_build(float t, unsigned band, int sms, cudaStream
     // the FP32 rounding of the distances
     const double rmax = 0.5 * w.gh * std::sqrt(static_cast<double>(w.dim)) * (1.0 + 1e-3);
     const float extra = static_cast<float>(2.0 * rmax + 8.0 * lattice_margin);
-    if ((e = launch_near_lists(w, tb, extra, static_cast<int *>(glist.ptr),
-                               static_cast<int *>(gpool.ptr), static_cast<int>(slots), count + 1,
-                               sms, stream)) != cudaSuccess) {
+    // list_prefix's buckets: the same rounding margin as the list radius
+    const float slack = static_cast<float>(8.0 * lattice_margin);
+    if ((e = launch_near_lists(w, tb, extra, static_cast<float>(rmax), slack,
+                               static_cast<int2 *>(glist.ptr), static_cast<int *>(gpool.ptr),
+                               static_cast<int>(slots), count + 1, sms, stream)) !=
+        cudaSuccess) {
         return e;
     }
-    if ((e = gaos.reserve(prim_aos_bytes(w))) != cudaSuccess) return e;
-    if ((e = launch_prim_aos(w, static_cast<float *>(gaos.ptr), stream)) != cudaSuccess) return e;
+    if (wide.aos == nullptr) {
+        if ((e = gaos.reserve(prim_aos_bytes(w))) != cudaSuccess) return e;
+        if ((e = launch_prim_aos(w, static_cast<float *>(gaos.ptr), stream)) != cudaSuccess) {
+            return e;
+        }
+    }
     wide.gk = w.gk;
-    wide.gl = static_cast<const int *>(glist.ptr);
+    wide.gl = static_cast<const int2 *>(glist.ptr);
+    wide.gbinv = static_cast<float>((kListBuckets + 1) / rmax);
     wide.gpool = static_cast<const int *>(gpool.ptr);
     wide.aos = static_cast<const float4 *>(gaos.ptr);
     list_built = tb;
@@ -318,6 +326,15 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
         if ((e = cudaMallocAsync(&skip, lattice_skip_bytes(wide), stream)) != cudaSuccess) return e;
     }
     const double tol = 1e-5 * std::max(mag, ext);
+    if (h.dim == 3) {
+        // the 3D tile build scans candidates from the contiguous records
+        // (kept for the near-boundary list scans)
+        if ((e = gaos.reserve(prim_aos_bytes(wide))) != cudaSuccess) return e;
+        if ((e = launch_prim_aos(wide, static_cast<float *>(gaos.ptr), stream)) != cudaSuccess) {
+            return e;
+        }
+        wide.aos = static_cast<const float4 *>(gaos.ptr);
+    }
     e = launch_lattice32(view, wide, margin, out, sms, skip, tol, stream);
     if (skip) {
         const cudaError_t f = cudaFreeAsync(skip, stream);

@@ -57,15 +57,23 @@ struct WideView {
     // D >= gratio * r, i.e. when it is at least (gratio - 1) / (gratio + 1)
     // of the upper bound D + r of the true distance
     float gratio;
-    // Near-boundary candidate lists (null when absent): gl[node] is -1 or
+    // Near-boundary candidate lists (null when absent): gl[node].x is -1 or
     // (offset << 5) | (length - 1), the list's wide slots at gpool + offset,
     // lists packed end to end (at most gk slots each).  The list holds every
     // primitive within d(node) + 2 r_max of the node (r_max the largest
     // distance from a point to its nearest node), so it holds the nearest
-    // primitive of every point whose nearest node this is.
-    const int *gl;
+    // primitive of every point whose nearest node this is.  2D lists (a few
+    // segments, scanned by one lane) keep ascending slot order and .y = 0.
+    // 3D lists (scanned by the warp) are ordered by their slots' distance D
+    // from the node, and gl[node].y packs, in 6 bits per bucket
+    // b < kListBuckets, how many have D <= d(node) + 2 rho_b (+ rounding
+    // slack), rho_b = (b + 1) r_max / (kListBuckets + 1): a point within
+    // rho_b of the node has its nearest primitive among those (list_prefix).
+    // gbinv = (kListBuckets + 1) / r_max.
+    const int2 *gl;
     const int *gpool;
     int gk;
+    float gbinv;
     // the primitive records again, one per wide slot, contiguous (2D: 5 of 8
     // floats, 3D: 16 floats), for the list scans' per-lane gathers
     const float4 *aos;
@@ -220,9 +228,24 @@ __device__ __forceinline__ const int *list_of(const WideView &w, int packed) {
 }
 __device__ __forceinline__ int list_length(int packed) { return (packed & 31) + 1; }
 
+// Distance buckets of a list entry (WideView::gl).
+constexpr int kListBuckets = 5;
+
+// The packed list entry of a query at distance r from its node, its length
+// cut to the entries that can hold the query's nearest primitive: with
+// r <= rho_b, those with D <= d(node) + 2 rho_b (the list's bucket b), since
+// the nearest primitive is within d(p) + r <= d(node) + 2 r of the node.
+// The minimum over that prefix is the minimum over the whole list.
+__device__ __forceinline__ int list_prefix(const WideView &w, int2 v, float r) {
+    const int b = min(static_cast<int>(r * w.gbinv), kListBuckets);
+    if (b == kListBuckets) return v.x;
+    const int k = max((v.y >> (6 * b)) & 63, 1);
+    return (v.x & ~31) | (k - 1);
+}
+
 // Closest primitive among a near-boundary candidate list of k wide slots,
 // found by this lane alone; the first minimum in list order (ascending
-// slots) wins.
+// slots: 2D lists keep slot order) wins.
 template <int DIM>
 __device__ __forceinline__ WideResult list_nearest(const WideView &w, const int *list, int k,
                                                    float px, float py, float pz) {
@@ -305,9 +328,9 @@ __device__ __forceinline__ WideResult warp_list_nearest(const WideView &w, bool 
 
 // Every primitive within squared FP32 distance r2 of (px, py, pz), found by
 // the whole warp (all lanes call it with the same point): the wide slots in
-// ascending order go to out[0 .. cap), the count (which may exceed cap) is
-// returned to every lane.  Children are visited when their lower bound
-// (box and slab) is within r2.
+// ascending order go to out[0 .. cap) and their count to every lane.  Once
+// more than cap are found the search stops and returns a count above cap.
+// Children are visited when their lower bound (box and slab) is within r2.
 template <int DIM>
 __device__ int wide_range(const WideView &w, float px, float py, float pz, float r2, int *out,
                           int cap) {
@@ -343,6 +366,7 @@ __device__ int wide_range(const WideView &w, float px, float py, float pz, float
         const int child = parent[h] * 32 + k;
         if (h == 1) {
             leaf(child);
+            if (count > cap) break;
         } else {
             --h;
             parent[h] = child;

@@ -259,8 +259,9 @@ cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaSt
 // scans: prim_aos_bytes(w) bytes.
 size_t prim_aos_bytes(const WideView &w);
 cudaError_t launch_prim_aos(const WideView &w, float *aos, cudaStream_t stream);
-cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
-                              int pool_slots, unsigned *counter, int sms, cudaStream_t stream);
+cudaError_t launch_near_lists(const WideView &w, float t, float extra, float rmax, float slack,
+                              int2 *gl, int *pool, int pool_slots, unsigned *counter, int sms,
+                              cudaStream_t stream);
 cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin, float *out,
                              int sms, void *scratch, double tol, cudaStream_t stream);
 // lattice_bound at each point (FP32), NaN where the scene has no lattice.

@@ -312,7 +312,8 @@ __global__ void __launch_bounds__(256, MIN_BLOCKS) heat_walk_kernel(HeatArgs a) 
                             // near the boundary: a query over the node's
                             // candidate list, when it has one (2D: this
                             // lane scans it; 3D: the warp, below)
-                            const int v = __ldg(wv.gl + ls.node);
+                            const int2 e = __ldg(wv.gl + ls.node);
+                            const int v = DIM == 3 && e.x >= 0 ? list_prefix(wv, e, ls.r) : e.x;
                             if (v >= 0) {
                                 if constexpr (DIM == 2) {
                                     const WideResult q = list_nearest<DIM>(

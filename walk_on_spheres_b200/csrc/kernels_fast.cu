@@ -103,7 +103,8 @@ __device__ __forceinline__ void fast_task(const FastArgs a, const WideView &wv, 
                             // candidate list, when it has one; in 2D (a
                             // few segments) this lane scans it, in 3D the
                             // warp scans all such lists together below
-                            const int v = __ldg(wv.gl + ls.node);
+                            const int2 e = __ldg(wv.gl + ls.node);
+                            const int v = DIM == 3 && e.x >= 0 ? list_prefix(wv, e, ls.r) : e.x;
                             if (v >= 0) {
                                 if constexpr (DIM == 2) {
                                     const WideResult q = list_nearest<DIM>(
@@ -661,56 +662,174 @@ __global__ void special32_kernel(const double *x, long long n, double *li0, doub
 }  // namespace
 
 namespace {
-// One lattice node per warp: the FP32 cooperative query at the node's FP32
-// position glo + (i, j, k) gh, the same position the walks' lattice_sample
-// rebuilds.  The query prunes conservatively (keep = (1 - tau)^2, as the
-// walks do above the shell): it returns a squared distance at most
-// 1 / keep times the true one, and a node deep inside a round mesh, nearly
-// equidistant from every primitive, does not visit them all.  So the value
-// stored is sqrt(best) (1 - tau) minus `margin` (the FP32 rounding of the
-// primitive distances, a few ulps of the coordinates), rounded down.
+// Whether lattice node (i, j, k) and its neighbours all lie outside the mesh
+// (the row-parity mask): such a node stores 0 (a valid lower bound, written
+// as -0.0 to mark the skip) without a query, since no walk inside the
+// domain samples it for a useful bound.
+template <int DIM>
+__device__ __forceinline__ bool node_skipped(const WideView &w, const uint8_t *outside, int i,
+                                             int j, int k) {
+    bool all_out = true;
+    for (int q = 0; q < (DIM == 2 ? 9 : 27) && all_out; ++q) {
+        const int ni = i + q % 3 - 1, nj = j + (q / 3) % 3 - 1;
+        const int nk = DIM == 3 ? k + q / 9 - 1 : 0;
+        if (ni >= 0 && ni < w.gn[0] && nj >= 0 && nj < w.gn[1] && nk >= 0 && nk < w.gn[2]) {
+            all_out = outside[(ni * w.gn[1] + nj) * w.gn[2] + nk] != 0;
+        }
+    }
+    return all_out;
+}
+
+// Lattice nodes 32 at a time per warp: each lane decodes one node and
+// decides whether it is skipped; the warp then runs the FP32 cooperative
+// query for each remaining node in turn, at the node's FP32 position
+// glo + (i, j, k) gh, the same position the walks' lattice_sample rebuilds.
+// The query prunes conservatively (keep = (1 - tau)^2, as the walks do
+// above the shell): it returns a squared distance at most 1 / keep times the
+// true one, and a node deep inside a round mesh, nearly equidistant from
+// every primitive, does not visit them all.  So the value stored is
+// sqrt(best) (1 - tau) minus `margin` (the FP32 rounding of the primitive
+// distances, a few ulps of the coordinates), rounded down.  Node indices fit
+// in 32 bits (at most 2048^2 in 2D, 256^3 in 3D).
 template <int DIM, int HC>
 __global__ void __launch_bounds__(256) lattice32_kernel(WideView w, float margin,
                                                         const uint8_t *__restrict__ outside,
                                                         float *out) {
     constexpr float kShrink = 1.0f - 0x1p-10f;
     const int lane = threadIdx.x & 31;
-    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
-    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
-    constexpr int kNeighbours = DIM == 2 ? 9 : 27;
-    for (long long t = warp; t < n; t += warps) {
-        const int k = static_cast<int>(t % w.gn[2]);
-        const long long r = t / w.gn[2];
-        const int j = static_cast<int>(r % w.gn[1]);
-        const int i = static_cast<int>(r / w.gn[1]);
-        if (outside != nullptr) {
-            // a node whose own and neighbours' centres are all outside the
-            // mesh stores 0 (a valid lower bound) without a query: no walk
-            // inside the domain samples it for a useful bound
-            bool out_n = true;
-            if (lane < kNeighbours) {
-                const int ni = i + lane % 3 - 1, nj = j + (lane / 3) % 3 - 1;
-                const int nk = DIM == 3 ? k + lane / 9 - 1 : 0;
-                if (ni >= 0 && ni < w.gn[0] && nj >= 0 && nj < w.gn[1] && nk >= 0 &&
-                    nk < w.gn[2]) {
-                    out_n = outside[(static_cast<long long>(ni) * w.gn[1] + nj) * w.gn[2] + nk] != 0;
-                }
+    const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    const int n = w.gn[0] * w.gn[1] * w.gn[2];
+    for (int base = warp * 32; base < n; base += warps * 32) {
+        const int t = base + lane;
+        bool query = t < n;
+        float x = 0.0f, y = 0.0f, z = 0.0f;
+        if (query) {
+            const int k = t % w.gn[2];
+            const int r = t / w.gn[2];
+            const int j = r % w.gn[1];
+            const int i = r / w.gn[1];
+            if (outside != nullptr && node_skipped<DIM>(w, outside, i, j, k)) {
+                out[t] = -0.0f;  // -0.0: a valid bound that marks the node as skipped
+                query = false;
             }
-            if (__all_sync(kFull, out_n)) {
-                // -0.0: a valid bound that marks the node as skipped
-                if (lane == 0) out[t] = -0.0f;
-                continue;
+            x = w.glo[0] + static_cast<float>(i) * w.gh;
+            y = w.glo[1] + static_cast<float>(j) * w.gh;
+            z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
+        }
+        unsigned pending = __ballot_sync(kFull, query);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1u;
+            const float qx = __shfl_sync(kFull, x, src);
+            const float qy = __shfl_sync(kFull, y, src);
+            const float qz = __shfl_sync(kFull, z, src);
+            const WideResult q = wide_nearest<DIM, HC>(w, qx, qy, qz, kShrink * kShrink, 0.0f);
+            if (lane == src) {
+                const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
+                out[t] = d > 0.0f ? d : 0.0f;
             }
         }
+    }
+}
+
+// 3D lattice by warp tiles of 2 x 4 x 4 nodes (i, j, k), one node per lane.
+// The nearest primitive of a node x lies within d(x) + |x - c| <= d(c) +
+// 2 |x - c| of the tile centre c, so every primitive within d(c) + 2 r_tile
+// (r_tile: the largest |x - c|, plus a rounding slack) is a candidate for
+// every node of the tile; the warp collects them once (kTileCap at most) and
+// each lane takes the FP32 minimum over the candidates for its node, the
+// candidates' contiguous records (w.aos) staged 32 at a time in shared
+// memory.  That minimum is the
+// unpruned FP32 query's, so each node stores a value at most, and mostly
+// exactly, lattice32_kernel's (same (1 - tau) factor and margin).  A tile
+// with more candidates (deep inside a large round mesh, where many
+// primitives are nearly equidistant) stops collecting them and queries its
+// nodes one at a time as lattice32_kernel does.  A candidate costs each
+// lane about two warp instructions' worth of its node's time, against about
+// 700 for a per-node tree query even on a small mesh.
+constexpr int kTileCap = 512;
+
+template <int HC>
+__global__ void __launch_bounds__(256) lattice_tile3_kernel(WideView w, float margin,
+                                                            float slack,
+                                                            const uint8_t *__restrict__ outside,
+                                                            float *out) {
+    __shared__ int s_cand[8][kTileCap];
+    __shared__ float4 s_rec[8][32][4];  // 32 candidate records per warp at a time
+    constexpr float kShrink = 1.0f - 0x1p-10f;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    const int tj = (w.gn[1] + 3) / 4, tk = (w.gn[2] + 3) / 4;
+    const int tiles = ((w.gn[0] + 1) / 2) * tj * tk;
+    for (int tile = warp; tile < tiles; tile += warps) {
+        const int i0 = 2 * (tile / (tj * tk)), j0 = 4 * ((tile / tk) % tj), k0 = 4 * (tile % tk);
+        const int i = i0 + (lane >> 4), j = j0 + ((lane >> 2) & 3), k = k0 + (lane & 3);
+        const bool valid = i < w.gn[0] && j < w.gn[1] && k < w.gn[2];
+        const int t = valid ? (i * w.gn[1] + j) * w.gn[2] + k : 0;
+        bool query = valid;
+        if (valid && outside != nullptr && node_skipped<3>(w, outside, i, j, k)) {
+            out[t] = -0.0f;
+            query = false;
+        }
+        const unsigned want = __ballot_sync(kFull, query);
+        if (!want) continue;
         const float x = w.glo[0] + static_cast<float>(i) * w.gh;
         const float y = w.glo[1] + static_cast<float>(j) * w.gh;
-        const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-        const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, kShrink * kShrink, 0.0f);
-        if (lane == 0) {
-            const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
-            out[t] = d > 0.0f ? d : 0.0f;
+        const float z = w.glo[2] + static_cast<float>(k) * w.gh;
+        // the tile's centre and reach over its nodes inside the lattice
+        const int ni = min(2, w.gn[0] - i0), nj = min(4, w.gn[1] - j0), nk = min(4, w.gn[2] - k0);
+        const float cx = w.glo[0] + (static_cast<float>(i0) + 0.5f * (ni - 1)) * w.gh;
+        const float cy = w.glo[1] + (static_cast<float>(j0) + 0.5f * (nj - 1)) * w.gh;
+        const float cz = w.glo[2] + (static_cast<float>(k0) + 0.5f * (nk - 1)) * w.gh;
+        const float rt = 0.5f * w.gh *
+                         sqrtf(static_cast<float>((ni - 1) * (ni - 1) + (nj - 1) * (nj - 1) +
+                                                  (nk - 1) * (nk - 1))) *
+                         (1.0f + 0x1p-10f);
+        // the conservative query's distance is at least the exact one, so
+        // its radius covers the candidates as well
+        const WideResult qc = wide_nearest<3, HC>(w, cx, cy, cz, kShrink * kShrink, 0.0f);
+        const float radius = (sqrtf(qc.best) + 2.0f * rt) * (1.0f + 0x1p-16f) + slack;
+        const int cnt = wide_range<3>(w, cx, cy, cz, radius * radius, s_cand[wib], kTileCap);
+        __syncwarp();
+        if (cnt <= kTileCap) {
+            // 32 records at a time: each lane fetches one (all in flight
+            // together), then every lane measures its node against all 32
+            float best = INFINITY;
+            for (int c0 = 0; c0 < cnt; c0 += 32) {
+                const int m = min(32, cnt - c0);
+                if (lane < m) {
+                    const int sl = s_cand[wib][c0 + lane];
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) s_rec[wib][lane][f] = __ldg(w.aos + 4 * sl + f);
+                }
+                __syncwarp();
+#pragma unroll 4
+                for (int q = 0; q < m; ++q) best = fminf(best, eberly32(x, y, z, s_rec[wib][q]));
+                __syncwarp();
+            }
+            if (query) {
+                const float d = (sqrtf(best) * kShrink - margin) * (1.0f - 0x1p-20f);
+                out[t] = d > 0.0f ? d : 0.0f;
+            }
+        } else {
+            unsigned pending = want;
+            while (pending) {
+                const int src = __ffs(pending) - 1;
+                pending &= pending - 1u;
+                const float qx = __shfl_sync(kFull, x, src);
+                const float qy = __shfl_sync(kFull, y, src);
+                const float qz = __shfl_sync(kFull, z, src);
+                const WideResult q = wide_nearest<3, HC>(w, qx, qy, qz, kShrink * kShrink, 0.0f);
+                if (lane == src) {
+                    const float d = (sqrtf(q.best) * kShrink - margin) * (1.0f - 0x1p-20f);
+                    out[t] = d > 0.0f ? d : 0.0f;
+                }
+            }
         }
+        __syncwarp();
     }
 }
 
@@ -877,48 +996,96 @@ __global__ void near_band_kernel(const float *__restrict__ gd, long long n, floa
 // One band node per warp: its exact FP32 distance d, then every primitive
 // within d + extra, kept as its list when there are at most K.  Lists are
 // packed end to end, so the pool holds about the average length per node
-// rather than K: what the walks touch stays small enough for L2.
+// rather than K: what the walks touch stays small enough for L2.  A 3D list's
+// slots are written in increasing (distance from the node, slot) order, and
+// the entry's .y holds the bucket counts of list_prefix: for bucket b the
+// entries with D <= d + 2 rho_b + slack, rho_b = (b + 1) rmax / (B + 1).
+// `slack` covers the FP32 rounding of D, d and the query's distances.  2D
+// lists keep ascending slot order and no buckets (one lane scans a few
+// segments; the cut did not pay there).
 template <int DIM, int HC>
 __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, float extra,
-                                                         int *gl, int *pool, int pool_slots,
+                                                         float rmax, float slack, int2 *gl,
+                                                         int *pool, int pool_slots,
                                                          unsigned *counter) {
     __shared__ int s_list[8][32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const long long warp = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const long long warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
-    const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
+    const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    const int n = w.gn[0] * w.gn[1] * w.gn[2];  // at most 2^24 nodes
     const int K = w.gk;
-    for (long long node = warp; node < n; node += warps) {
-        const float d = w.gd[node];
-        if (signbit(d) || d > t) {
-            if (lane == 0) gl[node] = -1;
-            continue;
+    // 32 nodes per warp: each lane tests one for the band, then the warp
+    // builds the band nodes' lists one after another
+    for (int base = warp * 32; base < n; base += warps * 32) {
+        bool in_band = false;
+        if (base + lane < n) {
+            const float d = w.gd[base + lane];
+            in_band = !(signbit(d) || d > t);
+            if (!in_band) gl[base + lane] = make_int2(-1, 0);
         }
-        const int k = static_cast<int>(node % w.gn[2]);
-        const long long r = node / w.gn[2];
-        const int j = static_cast<int>(r % w.gn[1]);
-        const int i = static_cast<int>(r / w.gn[1]);
-        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
-        const float y = w.glo[1] + static_cast<float>(j) * w.gh;
-        const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-        const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, 1.0f, 0.0f);
-        const float radius = sqrtf(q.best) * (1.0f + 0x1p-16f) + extra;
-        const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list[wib], K);
-        __syncwarp();
-        // the list goes to the next cnt slots of the pool (lists end to end)
-        int idx = -1;
-        if (cnt >= 1 && cnt <= K) {
-            unsigned at = 0;
-            if (lane == 0) at = atomicAdd(counter, static_cast<unsigned>(cnt));
-            at = __shfl_sync(kFull, at, 0);
-            // never short: the pool holds K slots per band node (at most 2^26)
-            if (static_cast<long long>(at) + cnt <= pool_slots) idx = static_cast<int>(at);
+        unsigned pending = __ballot_sync(kFull, in_band);
+        while (pending) {
+            const int node = base + __ffs(pending) - 1;
+            pending &= pending - 1u;
+            const int k = node % w.gn[2];
+            const int r = node / w.gn[2];
+            const int j = r % w.gn[1];
+            const int i = r / w.gn[1];
+            const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+            const float y = w.glo[1] + static_cast<float>(j) * w.gh;
+            const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
+            const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, 1.0f, 0.0f);
+            const float dn = sqrtf(q.best);
+            const float radius = dn * (1.0f + 0x1p-16f) + extra;
+            const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list[wib], K);
+            __syncwarp();
+            // the list goes to the next cnt slots of the pool (lists end to end)
+            int idx = -1;
+            if (cnt >= 1 && cnt <= K) {
+                unsigned at = 0;
+                if (lane == 0) at = atomicAdd(counter, static_cast<unsigned>(cnt));
+                at = __shfl_sync(kFull, at, 0);
+                // never short: the pool holds K slots per band node (at most 2^26)
+                if (static_cast<long long>(at) + cnt <= pool_slots) idx = static_cast<int>(at);
+            }
+            if (idx < 0) {
+                if (lane == 0) gl[node] = make_int2(-1, 0);
+                __syncwarp();
+                continue;
+            }
+            if constexpr (DIM == 2) {
+                // 2D: ascending slot order, no buckets
+                if (lane < cnt) pool[static_cast<long long>(idx) + lane] = s_list[wib][lane];
+                if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), 0);
+                __syncwarp();
+                continue;
+            }
+            // 3D: each entry's distance from the node, its rank in (distance,
+            // slot) order, and the bucket counts
+            const bool mine = lane < cnt;
+            const int s = mine ? s_list[wib][lane] : 0;
+            const float dd = mine ? sqrtf(slot_dist<DIM>(w, s, x, y, z)) : INFINITY;
+            const unsigned long long key =
+                mine ? (static_cast<unsigned long long>(__float_as_uint(dd)) << 32) |
+                           static_cast<unsigned>(s)
+                     : ~0ull;
+            int rank = 0;
+            for (int o = 0; o < cnt; ++o) rank += __shfl_sync(kFull, key, o) < key ? 1 : 0;
+            if (mine) pool[static_cast<long long>(idx) + rank] = s;
+            unsigned buckets = 0;
+#pragma unroll
+            for (int b = 0; b < kListBuckets; ++b) {
+                const float rho =
+                    rmax * static_cast<float>(b + 1) / static_cast<float>(kListBuckets + 1);
+                const float lim = (dn + 2.0f * rho) * (1.0f + 0x1p-16f) + slack;
+                const unsigned c = __popc(__ballot_sync(kFull, mine && dd <= lim));
+                buckets |= min(c, 63u) << (6 * b);
+            }
+            // packed entry: (offset << 5) | (length - 1), offset < 2^26
+            if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), static_cast<int>(buckets));
+            __syncwarp();
         }
-        if (idx >= 0 && lane < cnt) pool[static_cast<long long>(idx) + lane] = s_list[wib][lane];
-        // packed entry: (offset << 5) | (length - 1), offset < 2^26
-        if (lane == 0) gl[node] = idx >= 0 ? (idx << 5) | (cnt - 1) : -1;
-        __syncwarp();
     }
 }
 }  // namespace
@@ -955,20 +1122,21 @@ cudaError_t launch_near_band(const WideView &w, float t, unsigned *count, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_near_lists(const WideView &w, float t, float extra, int *gl, int *pool,
-                              int pool_slots, unsigned *counter, int sms, cudaStream_t stream) {
+cudaError_t launch_near_lists(const WideView &w, float t, float extra, float rmax, float slack,
+                              int2 *gl, int *pool, int pool_slots, unsigned *counter, int sms,
+                              cudaStream_t stream) {
     const long long n = static_cast<long long>(w.gn[0]) * w.gn[1] * w.gn[2];
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
-    const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
+    const long long blocks = std::min<long long>((n + 255) / 256, static_cast<long long>(sms) * 8);
     return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
         constexpr int HC = decltype(h)::value;
         if (w.dim == 2) {
             near_lists_kernel<2, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-                w, t, extra, gl, pool, pool_slots, counter);
+                w, t, extra, rmax, slack, gl, pool, pool_slots, counter);
         } else {
             near_lists_kernel<3, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
-                w, t, extra, gl, pool, pool_slots, counter);
+                w, t, extra, rmax, slack, gl, pool, pool_slots, counter);
         }
         return cudaGetLastError();
     });
@@ -1006,13 +1174,21 @@ cudaError_t launch_lattice32(const SceneView &s, const WideView &w, float margin
             w, tol, count, cross, outside);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    const long long blocks = std::min<long long>((n + 7) / 8, static_cast<long long>(sms) * 8);
+    const long long blocks = std::min<long long>((n + 255) / 256, static_cast<long long>(sms) * 8);
+    // 3D warp tiles of 32 nodes; their candidate radius carries 12 margins
+    // of FP32 rounding (the tile centre, the nodes and the distances)
+    const long long tiles = static_cast<long long>((w.gn[0] + 1) / 2) * ((w.gn[1] + 3) / 4) *
+                            ((w.gn[2] + 3) / 4);
+    const long long tblocks = std::min<long long>((tiles + 7) / 8, static_cast<long long>(sms) * 8);
     // compiled per traversal class, like the walk kernels
     return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
         constexpr int HC = decltype(h)::value;
         if (w.dim == 2) {
             lattice32_kernel<2, HC>
                 <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, outside, out);
+        } else if (w.aos != nullptr) {
+            lattice_tile3_kernel<HC><<<static_cast<unsigned>(tblocks), 256, 0, stream>>>(
+                w, margin, 12.0f * margin, outside, out);
         } else {
             lattice32_kernel<3, HC>
                 <<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, margin, outside, out);
