@@ -2,6 +2,7 @@
 
     python -m walk_on_spheres_b200.benchmarks [--workloads a,b] [--scale 1.0] [--tune]
     python -m walk_on_spheres_b200.benchmarks --batch [--scale 1.0]
+    python -m walk_on_spheres_b200.benchmarks --batch-setup [--reps 3]
     python -m walk_on_spheres_b200.benchmarks --heat [--scale 1.0]
     python -m walk_on_spheres_b200.benchmarks --transient [--scale 1.0]
     python -m walk_on_spheres_b200.benchmarks --stationary [--scale 1.0]
@@ -21,6 +22,9 @@ Workloads (synthetic meshes from walk_on_spheres_b200.meshes):
 
 `--batch` runs the 64-solve mixed batch (mixed_batch_specs) as one
 graph-captured launch sequence and, for comparison, solve by solve.
+`--batch-setup` times the same batch's set-up alone (mesh checks, tree
+builds, uploads, lattices, near-boundary lists) at 1/250 of the walks, the
+launches an ncu launch list of the set-up selects.
 `--heat`, `--transient` and `--stationary` run the Gaussian heat-source
 forward/adjoint workload and the reference's welding levels 2 and 1.
 
@@ -240,6 +244,38 @@ def run_batch(scale: float = 1.0, device: int = 0, sequential: bool = True,
     return out
 
 
+def run_batch_setup(reps: int = 3, device: int = 0, seed: int = 2024) -> dict:
+    """Wall time of the mixed batch's one-time set-up: add_mesh / add_solve
+    for the 64 solves, prepare (tree builds on the host threads, uploads,
+    lattices) and the first run's plan (near-boundary lists), with the walk
+    counts scaled by 1/250 so the run itself is short.  Repeated `reps` times
+    on one context after a warm-up solve."""
+    from .batch import Batch
+    specs = mixed_batch_specs(seed, 0.004)
+    built = [build_mesh(sp["mesh"]) for sp in specs]
+    s = Solver(device)
+    s.set_mesh(built[0])
+    s.solve_grid(specs[0]["equation"], 8, 8, N_walks=64, method="fast")
+    runs = []
+    for _ in range(reps):
+        b = Batch(s)
+        t0 = time.perf_counter()
+        for sp, m in zip(specs, built):
+            mid = b.add_mesh(m)
+            b.add_solve(mid, sp["equation"], *sp["grid"], **sp["params"])
+        t1 = time.perf_counter()
+        b.prepare()
+        t2 = time.perf_counter()
+        ms = b.run(use_graph=False)
+        t3 = time.perf_counter()
+        runs.append({"add_s": t1 - t0, "prepare_s": t2 - t1,
+                     "plan_s": (t3 - t2) - ms / 1000.0, "run_ms": ms})
+        b.close()
+    s.close()
+    return {"workload": "mixed_batch_64_setup", "meshes": len(built),
+            "prims_total": int(sum(m.prims.shape[0] for m in built)), "runs": runs}
+
+
 def run_heat(scale: float = 1.0, device: int = 0, seed: int = 7) -> dict:
     """The differentiable heat-source workload: 3D Gaussian source Q = 1e3,
     sigma = 2 mm, x0 at the centre of the top face of a 0.10 x 0.05 x 0.01 m
@@ -384,6 +420,9 @@ def main(argv=None) -> int:
                     help="autotune the FAST_FP32 schedule and leaf size first")
     ap.add_argument("--batch", action="store_true",
                     help="run the 64-solve mixed batch instead of the single solves")
+    ap.add_argument("--batch-setup", action="store_true",
+                    help="time the mixed batch's set-up alone (1/250 of the walks)")
+    ap.add_argument("--reps", type=int, default=3, help="repetitions of --batch-setup")
     ap.add_argument("--heat", action="store_true",
                     help="run the differentiable heat-source workload (Green and MIS)")
     ap.add_argument("--transient", action="store_true",
@@ -405,6 +444,9 @@ def main(argv=None) -> int:
         return 0
     if a.heat:
         print(json.dumps(run_heat(a.scale, a.device)), flush=True)
+        return 0
+    if a.batch_setup:
+        print(json.dumps(run_batch_setup(a.reps, a.device)), flush=True)
         return 0
     if a.batch:
         print(json.dumps(run_batch(a.scale, a.device)), flush=True)
