@@ -49,3 +49,39 @@ def test_small_meshes_have_no_lattice(solver):
     solver.set_mesh(meshes.circle(segments=32))
     b = solver.distance_bounds(np.zeros((3, 2)))
     assert np.all(np.isnan(b))
+
+
+@pytest.mark.parametrize("mname", ["sphere", "slab"])
+def test_cut_lists_keep_every_walk(solver, monkeypatch, mname):
+    """3D near-boundary lists are scanned only up to the entries that can be
+    nearest for the query's distance from its node (list_prefix).  The
+    minimum over that prefix is the minimum over the whole list, so every
+    walk takes the same steps as with whole lists (WOS_LIST_CUT=0): the
+    screened grid solve (walk kernel) and the heat forward pass (heat
+    kernel) match bit for bit."""
+    from walk_on_spheres_b200.heat import HeatProblem
+
+    m = meshes.uv_sphere() if mname == "sphere" else meshes.slab_box(target_triangles=20000)
+
+    def run():
+        solver.set_mesh(m)  # each upload rebuilds the lists on the first solve
+        if mname == "sphere":
+            r = solver.solve_grid("screened_poisson", 20, 20, 20, N_walks=256, seed=7,
+                                  alpha=10.0, method="fast")
+            return r.mean.ravel(), r.mean_steps.ravel(), r.counters
+        rng = np.random.default_rng(11)
+        probes = np.array([0.10, 0.05, 0.01]) * rng.uniform(0.001, 0.999, size=(512, 3))
+        heat = HeatProblem(solver, probes, N_walks=256, epsilon=1e-5, seed=3,
+                           source_mode="green", method="fast")
+        f = heat.forward(1e3, (0.05, 0.025, 0.01), 2e-3)
+        return f.mean, f.mean_steps, f.counters
+
+    cut = run()
+    monkeypatch.setenv("WOS_LIST_CUT", "0")
+    whole = run()
+    monkeypatch.delenv("WOS_LIST_CUT")
+    assert cut[2]["exact_queries"] > 0
+    assert cut[2]["total_steps"] == whole[2]["total_steps"]
+    assert cut[2]["exact_queries"] == whole[2]["exact_queries"]
+    assert np.array_equal(cut[1], whole[1], equal_nan=True)
+    assert np.array_equal(cut[0], whole[0], equal_nan=True)

@@ -232,6 +232,11 @@ cudaError_t SceneDevice::lists_build(float t, unsigned band, int sms, cudaStream
     wide.gk = w.gk;
     wide.gl = static_cast<const int2 *>(glist.ptr);
     wide.gbinv = static_cast<float>((kListBuckets + 1) / rmax);
+    if (const char *env = std::getenv("WOS_LIST_CUT")) {
+        // every query past the node itself scans its whole list (the cut
+        // never changes a query's answer; this checks that)
+        if (std::string(env) == "0") wide.gbinv = 0x1p100f;
+    }
     wide.gpool = static_cast<const int *>(gpool.ptr);
     wide.aos = static_cast<const float4 *>(gaos.ptr);
     list_built = tb;
