@@ -285,9 +285,11 @@ void SceneDevice::set_views(const HostScene &h) {
 // The distance lattice of the FAST_FP32 walks (device/wide.cuh): nodes
 // spaced h = (largest bbox extent) / (G - 1) over the bounding box, G = 2048
 // in 2D and 256 in 3D (16 MB and 64 MB for a square / cubic box), distances
-// from the exact FP32 cooperative query at the nodes' FP32 positions.
-// Meshes of at most lane_prims primitives query exactly at every step and get
-// none; WOS_BOUND_GRID=0 turns it off.
+// at the nodes' FP32 positions from the conservative FP32 cooperative query
+// (2D) or from warp tiles' candidate scans over the contiguous records,
+// which are made first (3D; launch_lattice32).  Meshes of at most lane_prims
+// primitives query exactly at every step and get none; WOS_BOUND_GRID=0
+// turns it off.
 cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) {
     wide.gd = nullptr;
     if (h.n_prims <= lane_prims(h.dim)) return cudaSuccess;
@@ -323,14 +325,6 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
         return e;
     }
     auto *out = static_cast<float *>(lattice.ptr);
-    // outside-node skip: its row crossings and node mask live in a
-    // stream-ordered temporary (WOS_LATTICE_SKIP=0 queries every node)
-    void *skip = nullptr;
-    const char *skip_env = std::getenv("WOS_LATTICE_SKIP");
-    if (!(skip_env && std::string(skip_env) == "0")) {
-        if ((e = cudaMallocAsync(&skip, lattice_skip_bytes(wide), stream)) != cudaSuccess) return e;
-    }
-    const double tol = 1e-5 * std::max(mag, ext);
     if (h.dim == 3) {
         // the 3D tile build scans candidates from the contiguous records
         // (kept for the near-boundary list scans)
@@ -340,6 +334,14 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
         }
         wide.aos = static_cast<const float4 *>(gaos.ptr);
     }
+    // outside-node skip: its row crossings and node mask live in a
+    // stream-ordered temporary (WOS_LATTICE_SKIP=0 queries every node)
+    void *skip = nullptr;
+    const char *skip_env = std::getenv("WOS_LATTICE_SKIP");
+    if (!(skip_env && std::string(skip_env) == "0")) {
+        if ((e = cudaMallocAsync(&skip, lattice_skip_bytes(wide), stream)) != cudaSuccess) return e;
+    }
+    const double tol = 1e-5 * std::max(mag, ext);
     e = launch_lattice32(view, wide, margin, out, sms, skip, tol, stream);
     if (skip) {
         const cudaError_t f = cudaFreeAsync(skip, stream);
