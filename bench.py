@@ -98,10 +98,10 @@ REF_STRIDE = 128
 # fields written: the same at any walk count), and the L2 peak the capture
 # implies (lts__t_bytes.sum.per_second over
 # lts__t_sectors.sum.pct_of_peak_sustained_elapsed).
-NCU_PER_STEP = {"uniform": {"issued": 9751093419 / 595062422, "l2_bytes": 28.298615e9 / 595062422},
-                "green": {"issued": 9584133994 / 595069594, "l2_bytes": 28.265767e9 / 595069594}}
-NCU_DRAM_BYTES_PER_LAUNCH = 22.2e6
-NCU_L2_PEAK_GBS = 2506.406 / 0.07227765
+NCU_PER_STEP = {"uniform": {"issued": 9703405858 / 595884179, "l2_bytes": 28.752065e9 / 595884179},
+                "green": {"issued": 9536526621 / 595900507, "l2_bytes": 28.762581e9 / 595900507}}
+NCU_DRAM_BYTES_PER_LAUNCH = 17.6e6
+NCU_L2_PEAK_GBS = 2527.816 / 0.07299269
 ISSUE_SLOTS_PER_SM_CYCLE = 4   # one warp instruction per SM sub-partition per cycle
 # Adjoint workload: 3D Gaussian heat source Q exp(-|x - x0|^2 / sigma^2) on a
 # 0.10 x 0.05 x 0.01 m slab of ~20k triangles, g = 0, 4096 probes uniform in
