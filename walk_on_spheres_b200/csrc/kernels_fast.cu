@@ -993,16 +993,83 @@ __global__ void near_band_kernel(const float *__restrict__ gd, long long n, floa
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
-// One band node per warp: its exact FP32 distance d, then every primitive
-// within d + extra, kept as its list when there are at most K.  Lists are
-// packed end to end, so the pool holds about the average length per node
-// rather than K: what the walks touch stays small enough for L2.  A 3D list's
-// slots are written in increasing (distance from the node, slot) order, and
-// the entry's .y holds the bucket counts of list_prefix: for bucket b the
-// entries with D <= d + 2 rho_b + slack, rho_b = (b + 1) rmax / (B + 1).
-// `slack` covers the FP32 rounding of D, d and the query's distances.  2D
-// lists keep ascending slot order and no buckets (one lane scans a few
-// segments; the cut did not pay there).
+// Bucket b's reach for list_prefix: a list entry at distance D from a node
+// at distance d counts in bucket b when D <= d + 2 rho_b + slack,
+// rho_b = (b + 1) rmax / (B + 1).
+__device__ __forceinline__ float bucket_reach(float dn, int b, float rmax, float slack) {
+    const float rho = rmax * static_cast<float>(b + 1) / static_cast<float>(kListBuckets + 1);
+    return (dn + 2.0f * rho) * (1.0f + 0x1p-16f) + slack;
+}
+
+// One band node's list, built by the whole warp (all lanes call it
+// converged with the same node at (x, y, z)): the node's exact FP32
+// distance d, then every primitive within d + extra, kept as its list when
+// there are at most K.  Lists are packed end to end, so the pool holds about
+// the average length per node rather than K: what the walks touch stays
+// small enough for L2.  A 3D list's slots are written in increasing
+// (distance from the node, slot) order, and the entry's .y holds the bucket
+// counts of list_prefix (bucket_reach); `slack` covers the FP32 rounding of
+// D, d and the query's distances.  2D lists keep ascending slot order and no
+// buckets (one lane scans a few segments; the cut did not pay there).
+template <int DIM, int HC>
+__device__ void warp_node_list(const WideView &w, int node, float x, float y, float z,
+                               float extra, float rmax, float slack, int2 *gl, int *pool,
+                               int pool_slots, unsigned *counter, int *s_list) {
+    const int lane = threadIdx.x & 31;
+    const int K = w.gk;
+    const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, 1.0f, 0.0f);
+    const float dn = sqrtf(q.best);
+    const float radius = dn * (1.0f + 0x1p-16f) + extra;
+    const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list, K);
+    __syncwarp();
+    // the list goes to the next cnt slots of the pool (lists end to end)
+    int idx = -1;
+    if (cnt >= 1 && cnt <= K) {
+        unsigned at = 0;
+        if (lane == 0) at = atomicAdd(counter, static_cast<unsigned>(cnt));
+        at = __shfl_sync(kFull, at, 0);
+        // never short: the pool holds K slots per band node (at most 2^26)
+        if (static_cast<long long>(at) + cnt <= pool_slots) idx = static_cast<int>(at);
+    }
+    if (idx < 0) {
+        if (lane == 0) gl[node] = make_int2(-1, 0);
+        __syncwarp();
+        return;
+    }
+    if constexpr (DIM == 2) {
+        // 2D: ascending slot order, no buckets
+        if (lane < cnt) pool[static_cast<long long>(idx) + lane] = s_list[lane];
+        if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), 0);
+        __syncwarp();
+        return;
+    }
+    // 3D: each entry's distance from the node, its rank in (distance, slot)
+    // order, and the bucket counts
+    const bool mine = lane < cnt;
+    const int s = mine ? s_list[lane] : 0;
+    const float dd = mine ? sqrtf(slot_dist<DIM>(w, s, x, y, z)) : INFINITY;
+    const unsigned long long key =
+        mine ? (static_cast<unsigned long long>(__float_as_uint(dd)) << 32) |
+                   static_cast<unsigned>(s)
+             : ~0ull;
+    int rank = 0;
+    for (int o = 0; o < cnt; ++o) rank += __shfl_sync(kFull, key, o) < key ? 1 : 0;
+    if (mine) pool[static_cast<long long>(idx) + rank] = s;
+    unsigned buckets = 0;
+#pragma unroll
+    for (int b = 0; b < kListBuckets; ++b) {
+        const float lim = bucket_reach(dn, b, rmax, slack);
+        const unsigned c = __popc(__ballot_sync(kFull, mine && dd <= lim));
+        buckets |= min(c, 63u) << (6 * b);
+    }
+    // packed entry: (offset << 5) | (length - 1), offset < 2^26
+    if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), static_cast<int>(buckets));
+    __syncwarp();
+}
+
+// Band nodes 32 at a time per warp: each lane tests one node for the band
+// (0 <= value <= t), then the warp builds the band nodes' lists one after
+// another (warp_node_list).
 template <int DIM, int HC>
 __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, float extra,
                                                          float rmax, float slack, int2 *gl,
@@ -1014,9 +1081,6 @@ __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, fl
     const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
     const int n = w.gn[0] * w.gn[1] * w.gn[2];  // at most 2^24 nodes
-    const int K = w.gk;
-    // 32 nodes per warp: each lane tests one for the band, then the warp
-    // builds the band nodes' lists one after another
     for (int base = warp * 32; base < n; base += warps * 32) {
         bool in_band = false;
         if (base + lane < n) {
@@ -1035,56 +1099,164 @@ __global__ void __launch_bounds__(256) near_lists_kernel(WideView w, float t, fl
             const float x = w.glo[0] + static_cast<float>(i) * w.gh;
             const float y = w.glo[1] + static_cast<float>(j) * w.gh;
             const float z = DIM == 3 ? w.glo[2] + static_cast<float>(k) * w.gh : 0.0f;
-            const WideResult q = wide_nearest<DIM, HC>(w, x, y, z, 1.0f, 0.0f);
-            const float dn = sqrtf(q.best);
-            const float radius = dn * (1.0f + 0x1p-16f) + extra;
-            const int cnt = wide_range<DIM>(w, x, y, z, radius * radius, s_list[wib], K);
-            __syncwarp();
-            // the list goes to the next cnt slots of the pool (lists end to end)
-            int idx = -1;
-            if (cnt >= 1 && cnt <= K) {
-                unsigned at = 0;
-                if (lane == 0) at = atomicAdd(counter, static_cast<unsigned>(cnt));
-                at = __shfl_sync(kFull, at, 0);
-                // never short: the pool holds K slots per band node (at most 2^26)
-                if (static_cast<long long>(at) + cnt <= pool_slots) idx = static_cast<int>(at);
+            warp_node_list<DIM, HC>(w, node, x, y, z, extra, rmax, slack, gl, pool, pool_slots,
+                                    counter, s_list[wib]);
+        }
+    }
+}
+
+// 3D lists by warp tiles of 2 x 4 x 4 nodes, one node per lane, as the 3D
+// lattice is built: a band node's list holds the primitives within
+// d(node) + extra of it, so every primitive within d(c) + 2 r_tile + extra of
+// the tile centre c (plus a rounding slack) is a candidate for every node of
+// the tile.  Each band lane takes its exact FP32 distance as the minimum over
+// the candidates, keeps those within its list radius (the same test as the
+// per-node range query, in the same ascending slot order), sorts them by
+// (distance, slot) and writes them with their bucket counts; the lanes'
+// lists take consecutive pool ranges from one atomic per tile.  A tile with
+// more than kTileCap candidates builds its band nodes' lists one by one
+// (warp_node_list).  Records come from the contiguous copy (w.aos), staged
+// 32 at a time in shared memory.
+template <int HC>
+__global__ void __launch_bounds__(256) near_lists_tile3_kernel(WideView w, float t, float extra,
+                                                               float rmax, float slack,
+                                                               int2 *gl, int *pool,
+                                                               int pool_slots,
+                                                               unsigned *counter) {
+    __shared__ int s_cand[8][kTileCap];
+    __shared__ float4 s_rec[8][32][4];
+    __shared__ int s_list[8][32];
+    constexpr float kShrink = 1.0f - 0x1p-10f;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    const int K = w.gk;
+    const int tj = (w.gn[1] + 3) / 4, tk = (w.gn[2] + 3) / 4;
+    const int tiles = ((w.gn[0] + 1) / 2) * tj * tk;
+    for (int tile = warp; tile < tiles; tile += warps) {
+        const int i0 = 2 * (tile / (tj * tk)), j0 = 4 * ((tile / tk) % tj), k0 = 4 * (tile % tk);
+        const int i = i0 + (lane >> 4), j = j0 + ((lane >> 2) & 3), k = k0 + (lane & 3);
+        const bool valid = i < w.gn[0] && j < w.gn[1] && k < w.gn[2];
+        const int node = valid ? (i * w.gn[1] + j) * w.gn[2] + k : 0;
+        bool in_band = false;
+        if (valid) {
+            const float d = w.gd[node];
+            in_band = !(signbit(d) || d > t);
+            if (!in_band) gl[node] = make_int2(-1, 0);
+        }
+        const unsigned want = __ballot_sync(kFull, in_band);
+        if (!want) continue;
+        const float x = w.glo[0] + static_cast<float>(i) * w.gh;
+        const float y = w.glo[1] + static_cast<float>(j) * w.gh;
+        const float z = w.glo[2] + static_cast<float>(k) * w.gh;
+        const int ni = min(2, w.gn[0] - i0), nj = min(4, w.gn[1] - j0), nk = min(4, w.gn[2] - k0);
+        const float cx = w.glo[0] + (static_cast<float>(i0) + 0.5f * (ni - 1)) * w.gh;
+        const float cy = w.glo[1] + (static_cast<float>(j0) + 0.5f * (nj - 1)) * w.gh;
+        const float cz = w.glo[2] + (static_cast<float>(k0) + 0.5f * (nk - 1)) * w.gh;
+        const float rt = 0.5f * w.gh *
+                         sqrtf(static_cast<float>((ni - 1) * (ni - 1) + (nj - 1) * (nj - 1) +
+                                                  (nk - 1) * (nk - 1))) *
+                         (1.0f + 0x1p-10f);
+        // the conservative query's distance is at least the exact one
+        const WideResult qc = wide_nearest<3, HC>(w, cx, cy, cz, kShrink * kShrink, 0.0f);
+        const float reach = (sqrtf(qc.best) + 2.0f * rt + extra) * (1.0f + 0x1p-16f) + slack;
+        const int cnt = wide_range<3>(w, cx, cy, cz, reach * reach, s_cand[wib], kTileCap);
+        __syncwarp();
+        if (cnt > kTileCap) {
+            unsigned pending = want;
+            while (pending) {
+                const int src = __ffs(pending) - 1;
+                pending &= pending - 1u;
+                warp_node_list<3, HC>(w, __shfl_sync(kFull, node, src),
+                                      __shfl_sync(kFull, x, src), __shfl_sync(kFull, y, src),
+                                      __shfl_sync(kFull, z, src), extra, rmax, slack, gl, pool,
+                                      pool_slots, counter, s_list[wib]);
             }
-            if (idx < 0) {
-                if (lane == 0) gl[node] = make_int2(-1, 0);
-                __syncwarp();
-                continue;
-            }
-            if constexpr (DIM == 2) {
-                // 2D: ascending slot order, no buckets
-                if (lane < cnt) pool[static_cast<long long>(idx) + lane] = s_list[wib][lane];
-                if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), 0);
-                __syncwarp();
-                continue;
-            }
-            // 3D: each entry's distance from the node, its rank in (distance,
-            // slot) order, and the bucket counts
-            const bool mine = lane < cnt;
-            const int s = mine ? s_list[wib][lane] : 0;
-            const float dd = mine ? sqrtf(slot_dist<DIM>(w, s, x, y, z)) : INFINITY;
-            const unsigned long long key =
-                mine ? (static_cast<unsigned long long>(__float_as_uint(dd)) << 32) |
-                           static_cast<unsigned>(s)
-                     : ~0ull;
-            int rank = 0;
-            for (int o = 0; o < cnt; ++o) rank += __shfl_sync(kFull, key, o) < key ? 1 : 0;
-            if (mine) pool[static_cast<long long>(idx) + rank] = s;
-            unsigned buckets = 0;
+            continue;
+        }
+        // pass 1: each node's exact FP32 distance, the minimum over the
+        // candidates (its nearest primitive is one of them)
+        float best = INFINITY;
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+            const int m = min(32, cnt - c0);
+            if (lane < m) {
+                const int sl = s_cand[wib][c0 + lane];
 #pragma unroll
+                for (int f = 0; f < 4; ++f) s_rec[wib][lane][f] = __ldg(w.aos + 4 * sl + f);
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int q = 0; q < m; ++q) best = fminf(best, eberly32(x, y, z, s_rec[wib][q]));
+            __syncwarp();
+        }
+        const float dn = sqrtf(best);
+        const float radius = dn * (1.0f + 0x1p-16f) + extra;
+        const float r2 = radius * radius;
+        // pass 2: the candidates within the node's list radius, ascending slots
+        int lst[32];
+        float ld[32];
+        int len = 0;
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+            const int m = min(32, cnt - c0);
+            if (lane < m) {
+                const int sl = s_cand[wib][c0 + lane];
+#pragma unroll
+                for (int f = 0; f < 4; ++f) s_rec[wib][lane][f] = __ldg(w.aos + 4 * sl + f);
+            }
+            __syncwarp();
+            for (int q = 0; q < m; ++q) {
+                const float d2 = eberly32(x, y, z, s_rec[wib][q]);
+                if (in_band && d2 <= r2) {
+                    if (len < K) {
+                        lst[len] = s_cand[wib][c0 + q];
+                        ld[len] = sqrtf(d2);
+                    }
+                    ++len;
+                }
+            }
+            __syncwarp();
+        }
+        // the lanes' lists take consecutive pool ranges
+        const int take = in_band && len >= 1 && len <= K ? len : 0;
+        int incl = take;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        unsigned first = 0;
+        if (lane == 0 && total > 0) first = atomicAdd(counter, static_cast<unsigned>(total));
+        first = __shfl_sync(kFull, first, 0);
+        const long long at = static_cast<long long>(first) + (incl - take);
+        // never short: the pool holds K slots per band node (at most 2^26)
+        const bool fits = take > 0 && at + take <= pool_slots;
+        if (in_band && !fits) gl[node] = make_int2(-1, 0);
+        if (fits) {
+            // (distance, slot) order, as warp_node_list's ranks give
+            for (int a = 1; a < take; ++a) {
+                const int sa = lst[a];
+                const float da = ld[a];
+                int b = a - 1;
+                while (b >= 0 && (ld[b] > da || (ld[b] == da && lst[b] > sa))) {
+                    lst[b + 1] = lst[b];
+                    ld[b + 1] = ld[b];
+                    --b;
+                }
+                lst[b + 1] = sa;
+                ld[b + 1] = da;
+            }
+            for (int a = 0; a < take; ++a) pool[at + a] = lst[a];
+            unsigned buckets = 0;
             for (int b = 0; b < kListBuckets; ++b) {
-                const float rho =
-                    rmax * static_cast<float>(b + 1) / static_cast<float>(kListBuckets + 1);
-                const float lim = (dn + 2.0f * rho) * (1.0f + 0x1p-16f) + slack;
-                const unsigned c = __popc(__ballot_sync(kFull, mine && dd <= lim));
+                const float lim = bucket_reach(dn, b, rmax, slack);
+                unsigned c = 0;
+                for (int a = 0; a < take; ++a) c += ld[a] <= lim ? 1u : 0u;
                 buckets |= min(c, 63u) << (6 * b);
             }
-            // packed entry: (offset << 5) | (length - 1), offset < 2^26
-            if (lane == 0) gl[node] = make_int2((idx << 5) | (cnt - 1), static_cast<int>(buckets));
-            __syncwarp();
+            gl[node] = make_int2((static_cast<int>(at) << 5) | (take - 1),
+                                 static_cast<int>(buckets));
         }
     }
 }
@@ -1129,10 +1301,16 @@ cudaError_t launch_near_lists(const WideView &w, float t, float extra, float rma
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
     const long long blocks = std::min<long long>((n + 255) / 256, static_cast<long long>(sms) * 8);
+    const long long tiles = static_cast<long long>((w.gn[0] + 1) / 2) * ((w.gn[1] + 3) / 4) *
+                            ((w.gn[2] + 3) / 4);
+    const long long tblocks = std::min<long long>((tiles + 7) / 8, static_cast<long long>(sms) * 8);
     return with_height_class(height_class(w.H), [&](auto h) -> cudaError_t {
         constexpr int HC = decltype(h)::value;
         if (w.dim == 2) {
             near_lists_kernel<2, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+                w, t, extra, rmax, slack, gl, pool, pool_slots, counter);
+        } else if (w.aos != nullptr) {
+            near_lists_tile3_kernel<HC><<<static_cast<unsigned>(tblocks), 256, 0, stream>>>(
                 w, t, extra, rmax, slack, gl, pool, pool_slots, counter);
         } else {
             near_lists_kernel<3, HC><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
