@@ -85,3 +85,32 @@ def test_cut_lists_keep_every_walk(solver, monkeypatch, mname):
     assert cut[2]["exact_queries"] == whole[2]["exact_queries"]
     assert np.array_equal(cut[1], whole[1], equal_nan=True)
     assert np.array_equal(cut[0], whole[0], equal_nan=True)
+
+
+def test_tile_lattice_stores_the_node_queries_values(solver, monkeypatch):
+    """3D lattices are built by warp tiles, each lane taking its node's
+    minimum over candidates shared by the tile; WOS_LATTICE_TILES=0 builds
+    them node by node with the conservative cooperative query.  The tile
+    value is the unpruned minimum, so it is never above the node query's,
+    and it equals it at almost every node."""
+    m = meshes.uv_sphere()
+    rng = np.random.default_rng(9)
+    solver.set_mesh(m)
+    lo = np.asarray(solver.bbox[0::2][:3])
+    hi = np.asarray(solver.bbox[1::2][:3])
+    step = np.max(hi - lo) / 255.0
+    n = np.ceil((hi - lo) / step).astype(int) + 1
+    idx = rng.integers(0, n, size=(20000, 3))
+    # the nodes' FP32 positions glo + i h, where the bound is the node value
+    pts = (lo.astype(np.float32)[None, :] + idx.astype(np.float32) * np.float32(step))
+    pts = pts.astype(np.float64)
+    tiles = solver.distance_bounds(pts)
+    monkeypatch.setenv("WOS_LATTICE_TILES", "0")
+    solver.set_mesh(m)
+    nodes = solver.distance_bounds(pts)
+    monkeypatch.delenv("WOS_LATTICE_TILES")
+    solver.set_mesh(m)
+    assert np.all(tiles <= nodes), np.max(tiles - nodes)
+    queried = nodes > 0
+    assert queried.sum() > 5000
+    assert (tiles[queried] == nodes[queried]).mean() >= 0.95

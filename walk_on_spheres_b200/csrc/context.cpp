@@ -325,9 +325,11 @@ cudaError_t SceneDevice::build_lattice(const HostScene &h, cudaStream_t stream) 
         return e;
     }
     auto *out = static_cast<float *>(lattice.ptr);
-    if (h.dim == 3) {
+    const char *tiles_env = std::getenv("WOS_LATTICE_TILES");
+    if (h.dim == 3 && !(tiles_env && std::string(tiles_env) == "0")) {
         // the 3D tile build scans candidates from the contiguous records
-        // (kept for the near-boundary list scans)
+        // (kept for the near-boundary list scans); WOS_LATTICE_TILES=0
+        // builds lattice and lists node by node instead
         if ((e = gaos.reserve(prim_aos_bytes(wide))) != cudaSuccess) return e;
         if ((e = launch_prim_aos(wide, static_cast<float *>(gaos.ptr), stream)) != cudaSuccess) {
             return e;
